@@ -1,0 +1,142 @@
+/* kifmm.h -- C ABI of the B200 KIFMM evaluation engine (libkifmm_b200.so).
+ *
+ * Drop-in boundary for the reference's FMM3d path
+ * (lexingying/Kernel-independent-fast-multipole-method).  Every entry point
+ * below names the reference interface it replaces.  Plain pointers and
+ * sizes only; no C++ or torch types.  Positions and normals are 3 x n
+ * column-major doubles (xyz interleaved per point), exactly the reference's
+ * DblNumMat(3, n) (common/nummat.hpp:79-83); densities are sdof values per
+ * point and potentials tdof values per point (fmm3d/fmm3d_eval.cpp:57-59,
+ * :229-230).
+ *
+ * Every call returns a kifmm_status; the reference's assert paths
+ * (iA/iC, common/commoninc.hpp:59-60) become codes.  A handle is owned by
+ * one caller; calls on distinct handles may come from different threads.
+ */
+#ifndef KIFMM_B200_H
+#define KIFMM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct kifmm_engine* kifmm_handle;
+
+typedef enum {
+  KIFMM_OK = 0,
+  KIFMM_ERR_ARG = 1,         /* null pointer, bad size or count */
+  KIFMM_ERR_KERNEL = 2,      /* kernel id not supported by FMM3d::setup (fmm3d/fmm3d_setup.cpp:41-54) */
+  KIFMM_ERR_OUT_OF_BOX = 3,  /* a point outside the root box (fmm3d/let3d.cpp:73,155) */
+  KIFMM_ERR_STATE = 4,       /* call order (eval before setup, geometry missing, ...) */
+  KIFMM_ERR_OPTION = 5,      /* missing or malformed -fmm3d_* option (fmm3d/fmm3d_setup.cpp:30, let3d.cpp:45-48) */
+  KIFMM_ERR_CUDA = 6,        /* a CUDA runtime error (message in kifmm_last_error) */
+  KIFMM_ERR_ALLOC = 7,       /* device or host allocation failed */
+  KIFMM_ERR_NUMERIC = 8,     /* operator precompute failed (e.g. SVD did not converge) */
+  KIFMM_ERR_NO_DEVICE = 9    /* no CUDA device: there is no CPU fallback */
+} kifmm_status;
+
+typedef enum {
+  KIFMM_PREC_FP64 = 0,   /* plain FP64 throughout (the reference's arithmetic) */
+  KIFMM_PREC_MIXED = 1   /* FP32 bulk sums and surface products; FP64 pseudo-inverses */
+} kifmm_precision;
+
+/* Replaces FMM3d::FMM3d(const string& prefix) (fmm3d/fmm3d.cpp:24-28).
+ * prefix is the option-key prefix ("fmm3d_" in fmm3d/tt.cpp:85). */
+kifmm_status kifmm_create(const char* prefix, kifmm_handle* out);
+
+/* Replaces FMM3d::~FMM3d (fmm3d/fmm3d.cpp:30-33). */
+kifmm_status kifmm_destroy(kifmm_handle h);
+
+/* Replaces KnlMat3d::srcpos()/srcnor()/trgpos() (fmm3d/knlmat3d.hpp:38-40).
+ * The arrays are read during kifmm_setup; unlike the reference the engine
+ * keeps its own copies afterwards. */
+kifmm_status kifmm_set_geometry(kifmm_handle h, int ns, const double* srcpos, const double* srcnor, int nt,
+                                const double* trgpos);
+
+/* Replaces KnlMat3d::knl() = Kernel3d(kt, coefs) (fmm3d/kernel3d.hpp:64).
+ * kt in {111,121,311,321,312,322,511,521}; coefs[0]=mu, coefs[1]=nu. */
+kifmm_status kifmm_set_kernel(kifmm_handle h, int kt, int ncoef, const double* coefs);
+
+/* Replaces FMM3d::ctr() and FMM3d::rootlvl() (fmm3d/fmm3d.hpp:73-74):
+ * root box centre and level (box radius 2^-rootlvl). */
+kifmm_status kifmm_set_box(kifmm_handle h, const double ctr[3], int rootlvl);
+
+/* One entry of the reference's option map (map<string,string>, fmm3d/tt.cpp:23-38).
+ * Keys the reference requires: -<prefix>np, -<prefix>let3d_ptsmax,
+ * -<prefix>let3d_maxlevel.  Engine keys: -<prefix>precision (fp64|mixed). */
+kifmm_status kifmm_set_option(kifmm_handle h, const char* key, const char* value);
+
+/* Replaces FMM3d::setup(map<string,string>&) (fmm3d/fmm3d_setup.cpp:26-63):
+ * octree, U/V/W/X lists (fmm3d/let3d.cpp:56-281), translation operators
+ * (fmm3d/matmgnt3d.cpp:91-361, built eagerly here), device buffers. */
+kifmm_status kifmm_setup(kifmm_handle h);
+
+/* Replaces FMM3d::eval(const DblNumVec& srcden, DblNumVec& trgval)
+ * (fmm3d/fmm3d_eval.cpp:24-243).  Host pointers: srcden has sdof*ns values,
+ * trgval receives tdof*nt values (overwritten, as :34 zeroes it). */
+kifmm_status kifmm_eval(kifmm_handle h, const double* srcden, double* trgval);
+
+/* Same evaluation for nrhs density vectors laid out one after another
+ * (srcden[r*sdof*ns + ...], trgval[r*tdof*nt + ...]).  Host pointers. */
+kifmm_status kifmm_eval_multi(kifmm_handle h, int nrhs, const double* srcden, double* trgval);
+
+/* Device-resident form: d_srcden / d_trgval are device pointers (double,
+ * same layout as kifmm_eval_multi); the work is enqueued on `stream`
+ * (a cudaStream_t, or NULL for the engine's own stream) and the call
+ * returns without synchronising when sync == 0. */
+kifmm_status kifmm_eval_device(kifmm_handle h, int nrhs, const double* d_srcden, double* d_trgval, void* stream,
+                               int sync);
+
+/* Replaces FMM3d::check(srcden, trgval, numchk) (fmm3d/fmm3d_check.cpp:25-73):
+ * FP64 direct sum at numchk targets picked with `seed`; returns
+ * ||fmm - direct|| / ||fmm|| in *relerr (the reference's metric, :61-71). */
+kifmm_status kifmm_check(kifmm_handle h, const double* srcden, const double* trgval, int numchk, uint64_t seed,
+                         double* relerr);
+
+/* Replaces Dense3d::eval (fmm3d/dense3d.cpp:38-57) on the device: FP64
+ * direct sum from the handle's sources to arbitrary targets (host arrays). */
+kifmm_status kifmm_direct(kifmm_handle h, const double* srcden, int nt, const double* trgpos, double* trgval);
+
+/* Tree introspection (Let3d, fmm3d/let3d.hpp:38-74), for list parity tests.
+ * Nodes are numbered exactly as the reference's breadth-first ndevec. */
+kifmm_status kifmm_tree_size(kifmm_handle h, int* nnodes, int* maxdepth);
+kifmm_status kifmm_tree_nodes(kifmm_handle h, int* depth, int* path, int* parent, int* child, int* tag,
+                              int* snum, int* tnum);
+/* which: 0=U 1=V 2=W 3=X.  total receives the list length sum; ptr (nnodes+1)
+ * and idx (total) may be NULL to query the size first. */
+kifmm_status kifmm_tree_lists(kifmm_handle h, int which, int64_t* total, int64_t* ptr, int* idx);
+/* Original point ids per node, grouped by leaf: 0=sources (sownvis) 1=targets (townvis). */
+kifmm_status kifmm_tree_points(kifmm_handle h, int which, int64_t* ptr, int* idx);
+
+/* sdof / tdof of the handle's kernel (Kernel3d::sdof/tdof, fmm3d/kernel3d.cpp:24-86). */
+kifmm_status kifmm_dofs(kifmm_handle h, int* sdof, int* tdof);
+
+/* Per-phase device times (ms) of the last eval, measured with CUDA events
+ * on the engine stream: [0] upward, [1] M2L, [2] X/S2L, [3] downward,
+ * [4] leaf (U/W/X/L2T), [5] total, and inside [1]: [6] forward spectra,
+ * [7] Hadamard accumulation, [8] inverse spectra.  n = entries written. */
+kifmm_status kifmm_phase_times(kifmm_handle h, double* ms, int* n);
+/* Enables (1) or disables (0) per-phase event timing (off by default). */
+kifmm_status kifmm_set_profiling(kifmm_handle h, int on);
+
+/* Work counters of the setup, for roofline accounting:
+ * [0] U-list point-point interactions, [1] V-list node pairs,
+ * [2] W/X direct interactions, [3] nodes, [4] leaves, [5] surface GEMM flops
+ * per eval, [6] forward spectra per eval, [7] inverse spectra per eval,
+ * [8] S2M + L2T + M2T + S2L point-surface interactions. */
+kifmm_status kifmm_work_counters(kifmm_handle h, double* counts, int* n);
+
+/* Number of this library's kernel launches issued by the last eval. */
+kifmm_status kifmm_last_launch_count(kifmm_handle h, int* nlaunch);
+
+const char* kifmm_status_string(kifmm_status s);
+/* Last error message of the handle (valid until the next call on it). */
+const char* kifmm_last_error(kifmm_handle h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

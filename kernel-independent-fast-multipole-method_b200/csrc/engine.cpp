@@ -1,0 +1,818 @@
+// FMM3d::setup / FMM3d::eval on one B200 (fmm3d/fmm3d_setup.cpp:26-140,
+// fmm3d/fmm3d_eval.cpp:24-243).  Host code: builds the tree and operators,
+// lays the per-level work lists and node data out in HBM once, and then
+// enqueues the evaluation passes on one stream:
+//
+//   load      scatter densities into leaf (Morton) order        eval.cpp:50-64
+//   upward    S2M P2P; per level bottom-up: UC2UE on leaves,
+//             fused M2M (UC2UE*UE2UC) on parents               eval.cpp:69-92
+//   V list    forward spectra, Hadamard accumulate, inverse    eval.cpp:115-150
+//   X list    S2L P2P to downward check surfaces               eval.cpp:176-191
+//   downward  per level top-down: DC2DE, fused L2L              eval.cpp:195-209
+//   leaves    U + W + X direct + M2T + L2T in one P2P pass     eval.cpp:98-111,154-172,210-213
+//   save      gather potentials back to the caller's order     eval.cpp:221-235
+#include "engine.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <random>
+#include <thread>
+
+#include "../../include/kifmm.h"
+#include "launch.hpp"
+
+namespace kifmm {
+
+namespace {
+
+int host_threads() {
+  unsigned n = std::thread::hardware_concurrency();
+  return n ? (int)std::min(n, 64u) : 4;
+}
+
+struct CudaError {
+  cudaError_t e;
+  const char* where;
+};
+
+#define KCHECK(call)                                      \
+  do {                                                    \
+    cudaError_t _e = (call);                              \
+    if (_e != cudaSuccess) throw CudaError{_e, #call};    \
+  } while (0)
+
+}  // namespace
+
+template <typename T>
+struct Impl : ImplBase {
+  Engine& E;
+  const Tree& tr;
+  const Operators& op;
+  std::vector<void*> allocs;
+
+  template <class U>
+  U* dalloc(size_t n) {
+    void* p = nullptr;
+    if (n == 0) n = 1;
+    KCHECK(cudaMalloc(&p, n * sizeof(U)));
+    allocs.push_back(p);
+    return (U*)p;
+  }
+  template <class U>
+  U* upload(const std::vector<U>& v) {
+    U* p = dalloc<U>(v.size());
+    if (!v.empty()) KCHECK(cudaMemcpy(p, v.data(), v.size() * sizeof(U), cudaMemcpyHostToDevice));
+    return p;
+  }
+  template <class U>
+  T* upload_as_T(const std::vector<U>& v) {
+    std::vector<T> t(v.size());
+    for (size_t i = 0; i < v.size(); i++) t[i] = (T)v[i];
+    return upload(t);
+  }
+
+  struct List {
+    int* work = nullptr;   // column / CTA node ids
+    int* aux = nullptr;    // second index list (GEMM B or C ids)
+    int n = 0;
+    int64_t* ptr = nullptr;
+    int* idx = nullptr;
+    int64_t* ptr2 = nullptr;
+    int* idx2 = nullptr;
+  };
+
+  int sd_u, td_u, sd_m, td_m, nsurf, nuc;
+  P2PArgs<T> args;
+  M2LGeom geom;
+  GemmScale scl;
+  // device buffers
+  int *d_sperm = nullptr, *d_tperm = nullptr, *d_path = nullptr, *d_depth = nullptr;
+  T *sden = nullptr, *tval = nullptr;
+  int cap_rhs = 0;
+  T *supeden, *supcval, *tdncval, *tdneden, *spectra, *effval;
+  double *A_uc2ue, *A_m2m, *A_dc2de, *A_l2l;  // FP64 in both precisions (see gemm.cu)
+  T* khat;
+  List s2m, s2l, leaf, m2l, fwd;
+  std::vector<List> up_leaf, up_non, dn, dn_par;
+  cudaEvent_t ev[9];  // phase boundaries + the two interior V-list kernel boundaries
+  bool have_events = false;
+  int nlaunch = 0;
+  double pt[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+
+  Impl(Engine& e) : E(e), tr(e.tree), op(*e.ops) {}
+  ~Impl() override {
+    for (void* p : allocs) cudaFree(p);
+    if (have_events)
+      for (auto& x : ev) cudaEventDestroy(x);
+  }
+
+  void build() {
+    sd_u = E.user.sd;
+    td_u = E.user.td;
+    sd_m = E.mm.sd;
+    td_m = E.mm.td;
+    nsurf = op.nsurf;
+    nuc = op.nuc;
+    const int nn = tr.nnodes;
+    // ---- node arrays
+    std::vector<int> chd = tr.chd;
+    args.nnodes = nn;
+    args.ns = E.ns;
+    args.nt = E.nt;
+    args.nsurf = nsurf;
+    args.nuc = nuc;
+    args.sbeg = upload(tr.sbeg);
+    args.scnt = upload(tr.scnt);
+    args.tbeg = upload(tr.tbeg);
+    args.tcnt = upload(tr.tcnt);
+    d_depth = upload(tr.depth);
+    args.depth = d_depth;
+    d_path = upload(tr.path);
+    args.center = upload(tr.center);
+    args.radius = upload(tr.radius);
+    d_sperm = upload(tr.sperm);
+    d_tperm = upload(tr.tperm);
+    // ---- points: coordinates relative to their leaf centre
+    std::vector<double> sl[6], tl[3];
+    for (auto& v : sl) v.assign(E.ns, 0.0);
+    for (auto& v : tl) v.assign(E.nt, 0.0);
+    for (int g = 0; g < nn; g++) {
+      if (!tr.terminal(g)) continue;
+      const double* c = &tr.center[3 * g];
+      for (int i = tr.sbeg[g]; i < tr.sbeg[g] + tr.scnt[g]; i++) {
+        int p = tr.sperm[i];
+        for (int d = 0; d < 3; d++) {
+          sl[d][i] = E.srcpos[3 * (size_t)p + d] - c[d];
+          sl[3 + d][i] = E.srcnor[3 * (size_t)p + d];
+        }
+      }
+      for (int i = tr.tbeg[g]; i < tr.tbeg[g] + tr.tcnt[g]; i++) {
+        int p = tr.tperm[i];
+        for (int d = 0; d < 3; d++) tl[d][i] = E.trgpos[3 * (size_t)p + d] - c[d];
+      }
+    }
+    args.sx = upload_as_T(sl[0]);
+    args.sy = upload_as_T(sl[1]);
+    args.sz = upload_as_T(sl[2]);
+    if (E.user.dl) {
+      args.snx = upload_as_T(sl[3]);
+      args.sny = upload_as_T(sl[4]);
+      args.snz = upload_as_T(sl[5]);
+    }
+    args.tx = upload_as_T(tl[0]);
+    args.ty = upload_as_T(tl[1]);
+    args.tz = upload_as_T(tl[2]);
+    // ---- surfaces and operators
+    args.ue_unit = upload_as_T(op.ue);
+    args.uc_unit = upload_as_T(op.uc);
+    args.de_unit = upload_as_T(op.de);
+    args.dc_unit = upload_as_T(op.dc);
+    A_uc2ue = upload(op.uc2ue);
+    A_m2m = upload(op.m2m);
+    A_dc2de = upload(op.dc2de);
+    A_l2l = upload(op.l2l);
+    {
+      std::vector<T> kh(op.m2l.size() * 2);
+      for (size_t i = 0; i < op.m2l.size(); i++) {
+        kh[2 * i] = (T)op.m2l[i].real();
+        kh[2 * i + 1] = (T)op.m2l[i].imag();
+      }
+      khat = upload(kh);
+    }
+    double kc[3];
+    kernel_constants(E.user.kt, E.user.coefs, kc);
+    args.ku = KConst<T>{(T)kc[0], (T)kc[1], (T)kc[2]};
+    kernel_constants(E.mm.kt, E.mm.coefs, kc);
+    args.km = KConst<T>{(T)kc[0], (T)kc[1], (T)kc[2]};
+    // ---- per-node data
+    supeden = dalloc<T>((size_t)nn * nsurf * sd_m);
+    KCHECK(cudaMemset(supeden, 0, sizeof(T) * (size_t)nn * nsurf * sd_m));  // empty nodes stay zero
+    supcval = dalloc<T>((size_t)nn * nuc * td_m);
+    tdncval = dalloc<T>((size_t)nn * nsurf * td_m);
+    tdneden = dalloc<T>((size_t)nn * nsurf * sd_m);
+    KCHECK(cudaMemset(tdneden, 0, sizeof(T) * (size_t)nn * nsurf * sd_m));
+    args.supeden = supeden;
+    args.supcval = supcval;
+    args.tdncval = tdncval;
+    args.tdneden = tdneden;
+
+    // ---- work lists
+    const int md = tr.maxdepth;
+    up_leaf.resize(md + 1);
+    up_non.resize(md + 1);
+    dn.resize(md + 1);
+    dn_par.resize(md + 1);
+    std::vector<int> v_s2m;
+    for (int d = 2; d <= md; d++) {
+      std::vector<int> ul, un, unc, dd, dp, dpc;
+      for (int g = tr.level_beg[d]; g < tr.level_beg[d + 1]; g++) {
+        if (tr.tag[g] & TAG_SRC) {
+          if (tr.terminal(g)) {
+            ul.push_back(g);
+            v_s2m.push_back(g);
+          } else {
+            un.push_back(g);
+            unc.push_back(tr.chd[g]);
+          }
+        }
+        if (tr.tag[g] & TAG_TRG) dd.push_back(g);
+      }
+      if (d >= 3)
+        for (int g = tr.level_beg[d - 1]; g < tr.level_beg[d]; g++)
+          if ((tr.tag[g] & TAG_TRG) && !tr.terminal(g)) {
+            dp.push_back(g);
+            dpc.push_back(tr.chd[g]);
+          }
+      up_leaf[d] = make_list(ul, {});
+      up_non[d] = make_list(un, unc);
+      dn[d] = make_list(dd, {});
+      dn_par[d] = make_list(dp, dpc);
+    }
+    s2m = make_list(v_s2m, {});
+    // V list (M2L), forward set
+    {
+      std::vector<int> work, fwdn;
+      std::vector<int64_t> ptr{0};
+      std::vector<int> idx;
+      std::vector<char> mark(nn, 0);
+      const Csr& V = tr.lists[1];
+      for (int g = 0; g < nn; g++) {
+        int64_t b = V.ptr[g], e = V.ptr[g + 1];
+        if (e == b) continue;
+        if (e - b > 192) throw CudaError{cudaErrorInvalidValue, "V list longer than 189"};
+        work.push_back(g);
+        for (int64_t k = b; k < e; k++) {
+          idx.push_back(V.idx[k]);
+          mark[V.idx[k]] = 1;
+        }
+        ptr.push_back((int64_t)idx.size());
+      }
+      for (int g = 0; g < nn; g++)
+        if (mark[g]) fwdn.push_back(g);
+      m2l = make_list(work, {}, ptr, idx);
+      fwd = make_list(fwdn, {});
+      effval = dalloc<T>((size_t)nn * td_m * op.nfreq * 2);
+      spectra = dalloc<T>((size_t)nn * sd_m * op.nfreq * 2);
+      // nodes outside every V list keep a zero spectrum (read by the parent-pair form)
+      KCHECK(cudaMemset(spectra, 0, sizeof(T) * (size_t)nn * sd_m * op.nfreq * 2));
+      counters_v = (double)idx.size();
+      if (sd_m == 1 && td_m == 1) build_pairs(work);
+      counters_fwd = (double)fwdn.size();
+      counters_inv = (double)work.size();
+    }
+    // X list (S2L when not direct), leaf work (U + direct W/X; M2T W)
+    {
+      std::vector<int> xw, lw;
+      std::vector<int64_t> xptr{0}, nptr{0}, mptr{0};
+      std::vector<int> xidx, nidx, midx;
+      const Csr& U = tr.lists[0];
+      const Csr& W = tr.lists[2];
+      const Csr& X = tr.lists[3];
+      double near_int = 0, surf_int = 0;
+      for (int g = 0; g < nn; g++) {
+        if (!(tr.tag[g] & TAG_TRG)) continue;
+        bool term = tr.terminal(g);
+        bool x_direct = term && (int64_t)tr.tcnt[g] * td_u < (int64_t)nsurf * td_m;  // fmm3d_eval.cpp:183
+        if (X.ptr[g + 1] > X.ptr[g] && !x_direct) {
+          xw.push_back(g);
+          for (int64_t k = X.ptr[g]; k < X.ptr[g + 1]; k++) {
+            xidx.push_back(X.idx[k]);
+            surf_int += (double)nsurf * tr.scnt[X.idx[k]];
+          }
+          xptr.push_back((int64_t)xidx.size());
+        }
+        if (!term) continue;
+        lw.push_back(g);
+        for (int64_t k = U.ptr[g]; k < U.ptr[g + 1]; k++) nidx.push_back(U.idx[k]);
+        for (int64_t k = W.ptr[g]; k < W.ptr[g + 1]; k++) {
+          int w = W.idx[k];
+          bool w_direct = tr.terminal(w) && (int64_t)tr.scnt[w] * sd_u < (int64_t)nsurf * sd_m;  // :161
+          if (w_direct)
+            nidx.push_back(w);
+          else
+            midx.push_back(w);
+        }
+        if (x_direct)
+          for (int64_t k = X.ptr[g]; k < X.ptr[g + 1]; k++) nidx.push_back(X.idx[k]);
+        for (int64_t k = nptr.back(); k < (int64_t)nidx.size(); k++) near_int += (double)tr.tcnt[g] * tr.scnt[nidx[k]];
+        surf_int += (double)tr.tcnt[g] * nsurf * ((int64_t)midx.size() - mptr.back() + (tr.depth[g] >= 2 ? 1 : 0));
+        nptr.push_back((int64_t)nidx.size());
+        mptr.push_back((int64_t)midx.size());
+      }
+      s2l = make_list(xw, {}, xptr, xidx);
+      leaf = make_list(lw, {}, nptr, nidx, mptr, midx);
+      for (int g : v_s2m) surf_int += (double)nuc * tr.scnt[g];
+      counters_near = near_int;
+      counters_surf = surf_int;
+    }
+    // ---- M2L geometry
+    geom.np = op.np;
+    geom.n = op.n;
+    geom.nh = op.nh;
+    geom.nfreq = op.nfreq;
+    geom.nsurf = nsurf;
+    geom.surf_ijk = upload(op.surf_ijk);
+    geom.sd = sd_m;
+    geom.td = td_m;
+    for (int s = 0; s < sd_m && s < 4; s++) geom.deg[s] = op.deg[s];
+    geom.rootlvl = E.rootlvl;
+    scl.sd = sd_m;
+    for (int s = 0; s < sd_m && s < 4; s++) scl.deg[s] = op.deg[s];
+    // GEMM flops per eval
+    double gf = 0;
+    for (int d = 2; d <= md; d++) {
+      gf += 2.0 * (nsurf * sd_m) * (nuc * td_m) * up_leaf[d].n;
+      gf += 2.0 * (nsurf * sd_m) * (8.0 * nsurf * sd_m) * up_non[d].n;
+      gf += 2.0 * (nsurf * sd_m) * (nsurf * td_m) * dn[d].n;
+      gf += 2.0 * (8.0 * nsurf * sd_m) * (nsurf * sd_m) * dn_par[d].n;
+    }
+    counters_gemm = gf;
+    for (auto& x : ev) KCHECK(cudaEventCreate(&x));
+    have_events = true;
+    ensure_rhs(1);
+  }
+
+  // Parent-pair form of the V list (single-dof equivalent kernels): one work
+  // item per target parent Q with its 26 colleague parents' first-child ids.
+  int pairs_n = 0, num_sms = 148;
+  int *pairs_chd = nullptr, *pairs_coll = nullptr;
+  unsigned char* pairs_mask = nullptr;
+  T* khat_c = nullptr;
+
+  void build_pairs(const std::vector<int>& vtargets) {
+    const Csr& V = tr.lists[1];
+    // compact offsets (max |o| >= 2) and the [dir][i][j] table
+    std::vector<int> compact(343, -1);
+    int nc = 0;
+    for (int ox = -3; ox <= 3; ox++)
+      for (int oy = -3; oy <= 3; oy++)
+        for (int oz = -3; oz <= 3; oz++)
+          if (std::max(std::abs(ox), std::max(std::abs(oy), std::abs(oz))) > 1) compact[offset_index(ox, oy, oz)] = nc++;
+    std::vector<short> tab(26 * 64, -1);
+    int dirs[26][3], nd = 0;
+    for (int dx = -1; dx <= 1; dx++)
+      for (int dy = -1; dy <= 1; dy++)
+        for (int dz = -1; dz <= 1; dz++)
+          if (dx || dy || dz) {
+            dirs[nd][0] = dx;
+            dirs[nd][1] = dy;
+            dirs[nd][2] = dz;
+            nd++;
+          }
+    for (int d = 0; d < 26; d++)
+      for (int i = 0; i < 8; i++)
+        for (int j = 0; j < 8; j++) {
+          int o[3];
+          for (int a = 0; a < 3; a++) o[a] = 2 * dirs[d][a] + ((j >> (2 - a)) & 1) - ((i >> (2 - a)) & 1);
+          if (std::max(std::abs(o[0]), std::max(std::abs(o[1]), std::abs(o[2]))) > 1)
+            tab[d * 64 + i * 8 + j] = (short)compact[offset_index(o[0], o[1], o[2])];
+        }
+    m2l_set_pair_table(tab.data(), nullptr);
+    KCHECK(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, E.device));
+    // one work item per target parent of a node with a V list
+    std::vector<int> qlist;
+    std::vector<char> seen(tr.nnodes, 0);
+    for (int t : vtargets) {
+      int q = tr.par[t];
+      if (!seen[q]) {
+        seen[q] = 1;
+        qlist.push_back(q);
+      }
+    }
+    std::sort(qlist.begin(), qlist.end());
+    std::vector<int> qchd, coll(qlist.size() * 26, -1);
+    std::vector<unsigned char> mask(qlist.size(), 0);
+    for (size_t w = 0; w < qlist.size(); w++) {
+      int q = qlist[w];
+      qchd.push_back(tr.chd[q]);
+      for (int i = 0; i < 8; i++) {
+        int t = tr.chd[q] + i;
+        if (V.ptr[t + 1] == V.ptr[t]) continue;
+        mask[w] |= (unsigned char)(1u << i);
+        for (int64_t k = V.ptr[t]; k < V.ptr[t + 1]; k++) {
+          int p = tr.par[V.idx[k]];
+          int dd[3];
+          for (int a = 0; a < 3; a++) dd[a] = tr.path[3 * p + a] - tr.path[3 * q + a];
+          int d = (dd[0] + 1) * 9 + (dd[1] + 1) * 3 + (dd[2] + 1);
+          if (d > 13) d--;  // skip (0,0,0)
+          coll[w * 26 + d] = tr.chd[p];
+        }
+      }
+    }
+    std::vector<T> kc((size_t)316 * op.nfreq * 2);
+    for (int oi = 0; oi < 343; oi++) {
+      if (compact[oi] < 0) continue;
+      for (int f = 0; f < op.nfreq; f++) {
+        kc[((size_t)compact[oi] * op.nfreq + f) * 2] = (T)op.m2l[(size_t)oi * op.nfreq + f].real();
+        kc[((size_t)compact[oi] * op.nfreq + f) * 2 + 1] = (T)op.m2l[(size_t)oi * op.nfreq + f].imag();
+      }
+    }
+    khat_c = upload(kc);
+    pairs_chd = upload(qchd);
+    pairs_coll = upload(coll);
+    pairs_mask = upload(mask);
+    pairs_n = (int)qlist.size();
+  }
+
+  double counters_v = 0, counters_fwd = 0, counters_inv = 0, counters_near = 0, counters_surf = 0,
+         counters_gemm = 0;
+
+  List make_list(const std::vector<int>& work, const std::vector<int>& aux, const std::vector<int64_t>& ptr = {},
+                 const std::vector<int>& idx = {}, const std::vector<int64_t>& ptr2 = {},
+                 const std::vector<int>& idx2 = {}) {
+    List l;
+    l.n = (int)work.size();
+    l.work = upload(work);
+    if (!aux.empty()) l.aux = upload(aux);
+    if (!ptr.empty()) {
+      l.ptr = upload(ptr);
+      l.idx = upload(idx);
+    }
+    if (!ptr2.empty()) {
+      l.ptr2 = upload(ptr2);
+      l.idx2 = upload(idx2);
+    }
+    return l;
+  }
+
+  void ensure_rhs(int nrhs) {
+    if (nrhs <= cap_rhs) return;
+    sden = dalloc<T>((size_t)nrhs * E.ns * sd_u);
+    tval = dalloc<T>((size_t)nrhs * E.nt * td_u);
+    cap_rhs = nrhs;
+    args.sden = sden;
+    args.tval = tval;
+  }
+
+  void gemm(int M, int K, const double* A, const T* B, int64_t ldb, const int* bidx, T* C, int64_t ldc, const int* cidx,
+            int ncol, bool acc, int out_lvl, bool in_on, int in_lvl, cudaStream_t st) {
+    if (ncol <= 0) return;
+    GemmScale s = scl;
+    s.out_on = 1;
+    s.out_lvl = out_lvl;
+    s.in_on = in_on ? 1 : 0;
+    s.in_lvl = in_lvl;
+    launch_node_gemm<T>(M, K, A, B, ldb, bidx, C, ldc, cidx, ncol, acc, s, st);
+    nlaunch++;
+  }
+
+  void p2p(const List& l, int which, int rhs, cudaStream_t st) {
+    if (l.n <= 0) return;
+    P2PWork w;
+    w.work = l.work;
+    w.n = l.n;
+    w.ptr = l.ptr;
+    w.idx = l.idx;
+    w.ptr2 = l.ptr2;
+    w.idx2 = l.idx2;
+    launch_p2p<T>(E.user.kt, args, w, which, rhs, st);
+    nlaunch++;
+  }
+
+  int eval(const double* d_srcden, double* d_trgval, int nrhs, cudaStream_t st) override {
+    ensure_rhs(nrhs);
+    nlaunch = 0;
+    const int md = tr.maxdepth, rl = E.rootlvl;
+    const int K1 = nsurf * sd_m;
+    bool prof = E.profiling;
+    if (prof) KCHECK(cudaEventRecord(ev[0], st));
+    launch_scatter_den<T>(d_srcden, d_sperm, E.ns, sd_u, nrhs, sden, st);
+    nlaunch++;
+    for (int r = 0; r < nrhs; r++) {
+      // upward
+      p2p(s2m, P2P_S2M, r, st);
+      for (int d = md; d >= 2; d--) {
+        const List& L = up_leaf[d];
+        gemm(K1, nuc * td_m, A_uc2ue, supcval, (int64_t)nuc * td_m, L.work, supeden, K1, L.work, L.n, false, d + rl,
+             false, 0, st);
+        const List& P = up_non[d];
+        gemm(K1, 8 * K1, A_m2m, supeden, K1, P.aux, supeden, K1, P.work, P.n, false, d + rl, true, d + 1 + rl, st);
+      }
+      if (prof && r == 0) KCHECK(cudaEventRecord(ev[1], st));
+      // V list
+      KCHECK(cudaMemsetAsync(tdncval, 0, sizeof(T) * (size_t)tr.nnodes * nsurf * td_m, st));
+      if (m2l.n > 0) {
+        launch_m2l_forward<T>(geom, supeden, fwd.work, fwd.n, d_depth, spectra, st);
+        if (prof && r == 0) KCHECK(cudaEventRecord(ev[7], st));
+        if (pairs_n > 0)
+          launch_m2l_hadamard_pairs<T>(op.nfreq, khat_c, spectra, pairs_n, pairs_chd, pairs_coll, pairs_mask, effval,
+                                       num_sms, st);
+        else
+          launch_m2l_hadamard<T>(geom, khat, spectra, m2l.work, m2l.n, m2l.ptr, m2l.idx, d_path, effval, st);
+        if (prof && r == 0) KCHECK(cudaEventRecord(ev[8], st));
+        launch_m2l_inverse<T>(geom, effval, m2l.work, m2l.n, tdncval, st);
+        nlaunch += 3;
+      }
+      if (prof && r == 0) KCHECK(cudaEventRecord(ev[2], st));
+      // X list
+      p2p(s2l, P2P_S2L, r, st);
+      if (prof && r == 0) KCHECK(cudaEventRecord(ev[3], st));
+      // downward
+      for (int d = 2; d <= md; d++) {
+        const List& L = dn[d];
+        gemm(K1, nsurf * td_m, A_dc2de, tdncval, (int64_t)nsurf * td_m, L.work, tdneden, K1, L.work, L.n, false, d + rl,
+             false, 0, st);
+        const List& P = dn_par[d];
+        gemm(8 * K1, K1, A_l2l, tdneden, K1, P.work, tdneden, K1, P.aux, P.n, true, d + rl, true, d - 1 + rl, st);
+      }
+      if (prof && r == 0) KCHECK(cudaEventRecord(ev[4], st));
+      // leaves
+      p2p(leaf, P2P_LEAF, r, st);
+      if (prof && r == 0) KCHECK(cudaEventRecord(ev[5], st));
+    }
+    launch_gather_val<T>(tval, d_tperm, E.nt, td_u, nrhs, d_trgval, st);
+    nlaunch++;
+    if (prof) {
+      KCHECK(cudaEventRecord(ev[6], st));
+      KCHECK(cudaEventSynchronize(ev[6]));
+      float ms;
+      for (int i = 0; i < 5; i++) {
+        KCHECK(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]));
+        pt[i] = ms;
+      }
+      KCHECK(cudaEventElapsedTime(&ms, ev[0], ev[6]));
+      pt[5] = ms;
+      if (m2l.n > 0) {
+        // ev[1] -> memset -> fwd -> ev[7] -> hadamard -> ev[8] -> inverse -> ev[2]
+        KCHECK(cudaEventElapsedTime(&ms, ev[1], ev[7]));
+        pt[6] = ms;
+        KCHECK(cudaEventElapsedTime(&ms, ev[7], ev[8]));
+        pt[7] = ms;
+        KCHECK(cudaEventElapsedTime(&ms, ev[8], ev[2]));
+        pt[8] = ms;
+      }
+    }
+    KCHECK(cudaGetLastError());
+    return KIFMM_OK;
+  }
+
+  void phase_times(double* ms) const override {
+    for (int i = 0; i < 9; i++) ms[i] = pt[i];
+  }
+  int launches() const override { return nlaunch; }
+};
+
+// ---------------------------------------------------------------------------
+Engine::~Engine() { release_device(); }
+
+void Engine::release_device() {
+  impl.reset();
+  double** bufs[] = {&d_in, &d_out, &d_spos, &d_snor, &d_sden, &d_tchk, &d_vchk};
+  for (double** b : bufs)
+    if (*b) {
+      cudaFree(*b);
+      *b = nullptr;
+    }
+  d_in_cap = d_out_cap = d_sden_cap = d_tchk_cap = 0;
+  if (stream) {
+    cudaStreamDestroy(stream);
+    stream = nullptr;
+  }
+}
+
+static bool parse_int(const std::map<std::string, std::string>& o, const std::string& key, int* v, bool* found) {
+  auto it = o.find(key);
+  *found = it != o.end();
+  if (!*found) return true;
+  const char* s = it->second.c_str();
+  char* end = nullptr;
+  long x = std::strtol(s, &end, 10);  // first token, like istringstream >> int
+  if (end == s) return false;
+  *v = (int)x;
+  return true;
+}
+
+int Engine::setup() {
+  ready = false;
+  if (!have_geom) {
+    err = "geometry not set (kifmm_set_geometry)";
+    return KIFMM_ERR_STATE;
+  }
+  if (!have_kernel) {
+    err = "kernel not set (kifmm_set_kernel)";
+    return KIFMM_ERR_STATE;
+  }
+  // options, FMM3d::setup (fmm3d/fmm3d_setup.cpp:30-31) and Let3d::setup (fmm3d/let3d.cpp:45-48)
+  bool f1, f2, f3;
+  if (!parse_int(opts, "-" + prefix + "np", &np, &f1) || !parse_int(opts, "-" + prefix + "let3d_ptsmax", &ptsmax, &f2) ||
+      !parse_int(opts, "-" + prefix + "let3d_maxlevel", &maxlevel, &f3)) {
+    err = "malformed option value";
+    return KIFMM_ERR_OPTION;
+  }
+  if (!f1 || !f2 || !f3) {
+    err = "missing required option (-" + prefix + "np, -" + prefix + "let3d_ptsmax, -" + prefix + "let3d_maxlevel)";
+    return KIFMM_ERR_OPTION;
+  }
+  if (np < 2 || np > 8) {
+    err = "np must be in [2, 8]";
+    return KIFMM_ERR_OPTION;
+  }
+  if (maxlevel < 1 || maxlevel > 21 || ptsmax < 1) {
+    err = "ptsmax must be >= 1 and maxlevel in [1, 21]";
+    return KIFMM_ERR_OPTION;
+  }
+  auto pit = opts.find("-" + prefix + "precision");
+  mixed = false;
+  if (pit != opts.end()) {
+    std::string v = pit->second;
+    v.erase(0, v.find_first_not_of(" \t"));
+    v = v.substr(0, v.find_first_of(" \t%"));
+    if (v == "mixed" || v == "fp32")
+      mixed = true;
+    else if (v != "fp64") {
+      err = "precision must be fp64 or mixed";
+      return KIFMM_ERR_OPTION;
+    }
+  }
+  if (!equivalent_kernel(user, &mm)) {
+    err = "kernel not supported by FMM3d";
+    return KIFMM_ERR_KERNEL;
+  }
+  release_device();
+  tree_ready = false;
+  // tree + lists
+  tree = Tree();
+  tree.ctr[0] = ctr[0];
+  tree.ctr[1] = ctr[1];
+  tree.ctr[2] = ctr[2];
+  tree.rootlvl = rootlvl;
+  tree.ptsmax = ptsmax;
+  tree.maxlevel = maxlevel;
+  int rc = build_tree(tree, ns, srcpos.data(), nt, trgpos.data(), host_threads(), &err);
+  if (rc == 3) return KIFMM_ERR_OUT_OF_BOX;
+  if (rc != 0) return KIFMM_ERR_OPTION;
+  tree_ready = true;
+  ops = get_operators(mm, np, host_threads(), &err);
+  if (!ops) return KIFMM_ERR_NUMERIC;
+  // device stage: there is no CPU fallback
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    err = "no CUDA device";
+    return KIFMM_ERR_NO_DEVICE;
+  }
+  cudaGetDevice(&device);
+  try {
+    if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess) throw CudaError{cudaGetLastError(), "stream"};
+    if (mixed) {
+      auto p = std::make_unique<Impl<float>>(*this);
+      p->build();
+      counters = {p->counters_near, p->counters_v, 0, (double)tree.nnodes, 0, p->counters_gemm, p->counters_fwd,
+                  p->counters_inv, p->counters_surf};
+      impl = std::move(p);
+    } else {
+      auto p = std::make_unique<Impl<double>>(*this);
+      p->build();
+      counters = {p->counters_near, p->counters_v, 0, (double)tree.nnodes, 0, p->counters_gemm, p->counters_fwd,
+                  p->counters_inv, p->counters_surf};
+      impl = std::move(p);
+    }
+    int nleaf = 0;
+    for (int g = 0; g < tree.nnodes; g++) nleaf += tree.terminal(g) && (tree.tag[g] & TAG_TRG);
+    counters[4] = nleaf;
+    KCHECK(cudaDeviceSynchronize());
+  } catch (const CudaError& e) {
+    err = std::string(e.where) + ": " + cudaGetErrorString(e.e);
+    cudaGetLastError();
+    release_device();
+    return e.e == cudaErrorMemoryAllocation ? KIFMM_ERR_ALLOC : KIFMM_ERR_CUDA;
+  }
+  ready = true;
+  return KIFMM_OK;
+}
+
+int Engine::eval_device(const double* d_srcden, double* d_trgval, int nrhs, cudaStream_t st, bool sync) {
+  if (!ready) {
+    err = "eval before a successful setup";
+    return KIFMM_ERR_STATE;
+  }
+  if (nrhs < 1 || (!d_srcden && ns > 0) || (!d_trgval && nt > 0)) {
+    err = "bad eval arguments";
+    return KIFMM_ERR_ARG;
+  }
+  if (!st) st = stream;
+  try {
+    int rc = impl->eval(d_srcden, d_trgval, nrhs, st);
+    if (rc != KIFMM_OK) return rc;
+    if (sync) KCHECK(cudaStreamSynchronize(st));
+  } catch (const CudaError& e) {
+    err = std::string(e.where) + ": " + cudaGetErrorString(e.e);
+    cudaGetLastError();
+    return KIFMM_ERR_CUDA;
+  }
+  return KIFMM_OK;
+}
+
+int Engine::eval_host(const double* srcden, double* trgval, int nrhs) {
+  if (!ready) {
+    err = "eval before a successful setup";
+    return KIFMM_ERR_STATE;
+  }
+  if (nrhs < 1 || (!srcden && ns > 0) || (!trgval && nt > 0)) {
+    err = "bad eval arguments";
+    return KIFMM_ERR_ARG;
+  }
+  size_t nin = (size_t)nrhs * ns * user.sd, nout = (size_t)nrhs * nt * user.td;
+  try {
+    if (nin > d_in_cap) {
+      if (d_in) cudaFree(d_in);
+      d_in = nullptr;
+      KCHECK(cudaMalloc(&d_in, std::max<size_t>(nin, 1) * sizeof(double)));
+      d_in_cap = nin;
+    }
+    if (nout > d_out_cap) {
+      if (d_out) cudaFree(d_out);
+      d_out = nullptr;
+      KCHECK(cudaMalloc(&d_out, std::max<size_t>(nout, 1) * sizeof(double)));
+      d_out_cap = nout;
+    }
+    KCHECK(cudaMemcpyAsync(d_in, srcden, nin * sizeof(double), cudaMemcpyHostToDevice, stream));
+    int rc = impl->eval(d_in, d_out, nrhs, stream);
+    if (rc != KIFMM_OK) return rc;
+    KCHECK(cudaMemcpyAsync(trgval, d_out, nout * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    KCHECK(cudaStreamSynchronize(stream));
+  } catch (const CudaError& e) {
+    err = std::string(e.where) + ": " + cudaGetErrorString(e.e);
+    cudaGetLastError();
+    return KIFMM_ERR_CUDA;
+  }
+  return KIFMM_OK;
+}
+
+int Engine::direct(const double* srcden, int ntc, const double* tpos, double* out) {
+  if (!ready) {
+    err = "direct before a successful setup";
+    return KIFMM_ERR_STATE;
+  }
+  try {
+    if (!d_spos) {
+      KCHECK(cudaMalloc(&d_spos, std::max<size_t>(1, 3 * (size_t)ns) * sizeof(double)));
+      KCHECK(cudaMalloc(&d_snor, std::max<size_t>(1, 3 * (size_t)ns) * sizeof(double)));
+      KCHECK(cudaMemcpy(d_spos, srcpos.data(), 3 * (size_t)ns * sizeof(double), cudaMemcpyHostToDevice));
+      KCHECK(cudaMemcpy(d_snor, srcnor.data(), 3 * (size_t)ns * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    size_t nden = (size_t)ns * user.sd;
+    if (nden > d_sden_cap || !d_sden) {
+      if (d_sden) cudaFree(d_sden);
+      d_sden = nullptr;
+      KCHECK(cudaMalloc(&d_sden, std::max<size_t>(1, nden) * sizeof(double)));
+      d_sden_cap = nden;
+    }
+    KCHECK(cudaMemcpy(d_sden, srcden, nden * sizeof(double), cudaMemcpyHostToDevice));
+    size_t ntp = std::max<size_t>(1, (size_t)ntc);
+    if (ntp > d_tchk_cap || !d_tchk) {
+      if (d_tchk) cudaFree(d_tchk);
+      if (d_vchk) cudaFree(d_vchk);
+      d_tchk = d_vchk = nullptr;
+      KCHECK(cudaMalloc(&d_tchk, 3 * ntp * sizeof(double)));
+      KCHECK(cudaMalloc(&d_vchk, 4 * ntp * sizeof(double)));
+      d_tchk_cap = ntp;
+    }
+    KCHECK(cudaMemcpy(d_tchk, tpos, 3 * (size_t)ntc * sizeof(double), cudaMemcpyHostToDevice));
+    double kc[3];
+    kernel_constants(user.kt, user.coefs, kc);
+    launch_direct(user.kt, d_spos, d_snor, d_sden, ns, d_tchk, ntc, d_vchk, kc, stream);
+    KCHECK(cudaGetLastError());
+    KCHECK(cudaMemcpyAsync(out, d_vchk, (size_t)ntc * user.td * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    KCHECK(cudaStreamSynchronize(stream));
+  } catch (const CudaError& e) {
+    err = std::string(e.where) + ": " + cudaGetErrorString(e.e);
+    cudaGetLastError();
+    return KIFMM_ERR_CUDA;
+  }
+  return KIFMM_OK;
+}
+
+int Engine::check(const double* srcden, const double* trgval, int numchk, uint64_t seed, double* relerr) {
+  if (!ready) {
+    err = "check before a successful setup";
+    return KIFMM_ERR_STATE;
+  }
+  if (numchk < 1 || nt < 1) {
+    err = "numchk and the target count must be positive";
+    return KIFMM_ERR_ARG;
+  }
+  // FMM3d::check picks targets uniformly at random (fmm3d/fmm3d_check.cpp:33-36)
+  std::mt19937_64 rng(seed);
+  std::vector<int> pick(numchk);
+  std::vector<double> tp(3 * (size_t)numchk), dv((size_t)numchk * user.td);
+  for (int k = 0; k < numchk; k++) {
+    pick[k] = (int)(rng() % (uint64_t)nt);
+    for (int d = 0; d < 3; d++) tp[3 * k + d] = trgpos[3 * (size_t)pick[k] + d];
+  }
+  int rc = direct(srcden, numchk, tp.data(), dv.data());
+  if (rc != KIFMM_OK) return rc;
+  double vn = 0, en = 0;  // :61-69
+  for (int k = 0; k < numchk; k++)
+    for (int i = 0; i < user.td; i++) {
+      double f = trgval[(size_t)pick[k] * user.td + i];
+      double dd = dv[(size_t)k * user.td + i] - f;
+      vn += f * f;
+      en += dd * dd;
+    }
+  *relerr = std::sqrt(en) / std::sqrt(vn);
+  return KIFMM_OK;
+}
+
+}  // namespace kifmm

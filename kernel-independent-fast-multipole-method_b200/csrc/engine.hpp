@@ -1,0 +1,67 @@
+// The evaluation engine behind the C ABI: one FMM3d-equivalent object.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "operators.hpp"
+#include "tree.hpp"
+
+namespace kifmm {
+
+struct ImplBase {
+  virtual ~ImplBase() = default;
+  // device-resident densities/potentials (double, original point order)
+  virtual int eval(const double* d_srcden, double* d_trgval, int nrhs, cudaStream_t st) = 0;
+  virtual void phase_times(double* ms) const = 0;
+  virtual int launches() const = 0;
+};
+
+struct Engine {
+  std::string prefix = "fmm3d_";
+  std::map<std::string, std::string> opts;
+  // geometry (host copies)
+  int ns = 0, nt = 0;
+  std::vector<double> srcpos, srcnor, trgpos;
+  bool have_geom = false;
+  KernelDesc user, mm;
+  bool have_kernel = false;
+  double ctr[3] = {0, 0, 0};
+  int rootlvl = 0;
+  // options
+  int np = 6, ptsmax = 150, maxlevel = 10;
+  bool mixed = false;
+  bool profiling = false;
+  // state
+  bool ready = false;       // device state built, eval allowed
+  bool tree_ready = false;  // host tree + lists built (introspection allowed)
+  std::string err;
+  Tree tree;
+  std::shared_ptr<const Operators> ops;
+  std::unique_ptr<ImplBase> impl;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  // work counters (kifmm_work_counters)
+  std::vector<double> counters;
+  // host-API staging (grown on demand)
+  double* d_in = nullptr;
+  double* d_out = nullptr;
+  size_t d_in_cap = 0, d_out_cap = 0;
+  // original-order copies for the direct sum (uploaded on first use)
+  double *d_spos = nullptr, *d_snor = nullptr, *d_sden = nullptr, *d_tchk = nullptr, *d_vchk = nullptr;
+  size_t d_sden_cap = 0, d_tchk_cap = 0;
+
+  ~Engine();
+  int setup();  // returns a kifmm_status
+  int eval_host(const double* srcden, double* trgval, int nrhs);
+  int eval_device(const double* d_srcden, double* d_trgval, int nrhs, cudaStream_t st, bool sync);
+  int direct(const double* srcden, int nt_chk, const double* tpos, double* out);
+  int check(const double* srcden, const double* trgval, int numchk, uint64_t seed, double* relerr);
+  void release_device();
+};
+
+}  // namespace kifmm

@@ -1,0 +1,99 @@
+// Host-callable launchers of the device passes (one stream argument each;
+// no synchronisation inside).  Argument structs hold device pointers only.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "kernels_common.cuh"
+
+namespace kifmm {
+
+// Device view of the tree, points and per-node surface data of one engine.
+template <typename T>
+struct P2PArgs {
+  int nnodes = 0, ns = 0, nt = 0, nsurf = 0, nuc = 0;
+  const int *sbeg = nullptr, *scnt = nullptr, *tbeg = nullptr, *tcnt = nullptr, *depth = nullptr;
+  const double *center = nullptr, *radius = nullptr;
+  // sorted points, coordinates relative to their leaf centre
+  const T *sx = nullptr, *sy = nullptr, *sz = nullptr, *snx = nullptr, *sny = nullptr, *snz = nullptr;
+  const T* sden = nullptr;  // [rhs][ns][sd]
+  const T *tx = nullptr, *ty = nullptr, *tz = nullptr;
+  T* tval = nullptr;  // [rhs][nt][td]
+  // unit surface grids (3 per point): UE radius 1, UC radius 3, DE radius 3, DC radius 1
+  const T *ue_unit = nullptr, *uc_unit = nullptr, *de_unit = nullptr, *dc_unit = nullptr;
+  // per-node surface data [node][point][dof] (one density vector at a time)
+  const T* supeden = nullptr;
+  const T* tdneden = nullptr;
+  T* supcval = nullptr;
+  T* tdncval = nullptr;
+  KConst<T> ku{}, km{};  // user and equivalent kernel constants
+};
+
+enum { P2P_S2M = 0, P2P_S2L = 1, P2P_LEAF = 2 };
+
+struct P2PWork {
+  const int* work = nullptr;  // node ids, one CTA each
+  int n = 0;
+  const int64_t* ptr = nullptr;  // CSR over work items (S2L: X leaves; LEAF: point-source leaves)
+  const int* idx = nullptr;
+  const int64_t* ptr2 = nullptr;  // LEAF: M2T source nodes
+  const int* idx2 = nullptr;
+};
+
+template <typename T>
+void launch_p2p(int kt, const P2PArgs<T>& a, const P2PWork& w, int which, int rhs, cudaStream_t st);
+
+void launch_direct(int kt, const double* spos, const double* snor, const double* sden, int ns, const double* tpos,
+                   int nt, double* out, const double* kc3, cudaStream_t st);
+
+template <typename T>
+void launch_scatter_den(const double* srcden, const int* perm, int ns, int sd, int nrhs, T* out, cudaStream_t st);
+template <typename T>
+void launch_gather_val(const T* tval, const int* perm, int nt, int td, int nrhs, double* trgval, cudaStream_t st);
+
+// Batched node GEMM: for j < ncol,
+//   C[cidx[j]*ldc + r] (=|+=) rs(r) * sum_k A[r*K + k] * ks(k) * B[bidx[j]*ldb + k]
+// with rs(r) = 2^(-out_lvl*deg[r % sd]) and ks(k) = 2^(in_lvl*deg[k % sd])
+// when the respective scaling is enabled.  A is M x K row-major.
+struct GemmScale {
+  int sd = 1;
+  int deg[4] = {0, 0, 0, 0};
+  int out_on = 0, out_lvl = 0;
+  int in_on = 0, in_lvl = 0;
+};
+
+template <typename T>
+void launch_node_gemm(int M, int K, const double* A, const T* B, int64_t ldb, const int* bidx, T* C, int64_t ldc,
+                      const int* cidx, int ncol, bool accumulate, const GemmScale& sc, cudaStream_t st);
+
+// FFT-based M2L (MatMgnt3d::plnden2effden / UE2DC_dgemv / effval2plnval,
+// fmm3d/matmgnt3d.cpp:223-361).
+struct M2LGeom {
+  int np = 0, n = 0, nh = 0, nfreq = 0, nsurf = 0;
+  const int* surf_ijk = nullptr;  // device, 3 per surface point
+  int sd = 1, td = 1;
+  int deg[4] = {0, 0, 0, 0};
+  int rootlvl = 0;
+};
+
+// spectra[node][s][f] (complex, interleaved re/im) of 2^(l*deg) * supeden[node]
+template <typename T>
+void launch_m2l_forward(const M2LGeom& g, const T* supeden, const int* nodes, int nnodes_work, const int* depth,
+                        T* spectra, cudaStream_t st);
+// effval[w][t][f] = sum_{s in V(work[w])} Khat[offset] * spectra[s]
+template <typename T>
+void launch_m2l_hadamard(const M2LGeom& g, const T* khat, const T* spectra, const int* work, int nwork,
+                         const int64_t* vptr, const int* vidx, const int* path, T* effval, cudaStream_t st);
+// Parent-pair form for single-dof kernels: effval[child of Q] for the nq target
+// parents, operator spectra in compact [316][nfreq] order (see m2l.cu).
+template <typename T>
+void launch_m2l_hadamard_pairs(int nf, const T* khat_c, const T* spectra, int nq, const int* qchd, const int* coll,
+                               const unsigned char* mask, T* effval, int num_sms, cudaStream_t st);
+void m2l_set_pair_table(const short* tab, cudaStream_t st);
+// tdncval[node] += extract(inverse(effval[node]))
+template <typename T>
+void launch_m2l_inverse(const M2LGeom& g, const T* effval, const int* work, int nwork, T* tdncval,
+                        cudaStream_t st);
+
+}  // namespace kifmm

@@ -1,0 +1,396 @@
+// FFT-accelerated M2L (V list), the reference's dominant phase
+// (fmm3d/fmm3d_eval.cpp:115-150; MatMgnt3d::plnden2effden, UE2DC_dgemv,
+// effval2plnval, fmm3d/matmgnt3d.cpp:223-361).
+//
+// The surface density of a node is a sparse (2np)^3 grid: only the np^3
+// corner block holds data, and only on its boundary.  Instead of a general
+// FFT library the transforms are pruned separable DFTs done in shared
+// memory, one CTA per node:
+//   forward : x pass (np^2 lines, np inputs -> np+1 outputs), y pass, z pass
+//   inverse : z and y passes evaluated only at the np outputs the surface
+//             needs, then the Hermitian half-line c2r along x at the surface
+//             points only.
+// The kernel spectra are computed once on the host (operators.cpp) with the
+// same sign convention w = exp(-2 pi i / n) and already carry 1/n^3.
+// Density and potential grids use indices [0, np) per axis; the reference's
+// np/2 shift (matmgnt3d.cpp:256) cancels between embedding and extraction.
+#include <algorithm>
+
+#include "launch.hpp"
+
+namespace kifmm {
+namespace {
+
+constexpr int FFT_THREADS = 256;
+constexpr int NPMAX = 8, NMAX = 16, NHMAX = 9;
+
+template <typename T>
+struct Cpx {
+  T re, im;
+};
+
+template <typename T>
+__device__ __forceinline__ void twiddles(Cpx<T>* w, int n) {
+  for (int m = threadIdx.x; m < n; m += blockDim.x) {
+    double s, c;
+    sincospi(-2.0 * (double)m / (double)n, &s, &c);
+    w[m].re = (T)c;
+    w[m].im = (T)s;
+  }
+}
+
+// spectra[node][s][f], f = (kz*n + ky)*nh + kx
+template <typename T>
+__global__ void __launch_bounds__(FFT_THREADS) k_m2l_fwd(M2LGeom g, const T* __restrict__ supeden,
+                                                          const int* __restrict__ nodes, const int* __restrict__ depth,
+                                                          T* __restrict__ spectra) {
+  __shared__ T xg[NPMAX * NPMAX * NPMAX];
+  __shared__ Cpx<T> A[NPMAX * NPMAX * NHMAX];  // A[k][j][kx]
+  __shared__ Cpx<T> Bm[NPMAX * NMAX * NHMAX];  // B[k][ky][kx]
+  __shared__ Cpx<T> w[NMAX];
+  const int np = g.np, n = g.n, nh = g.nh, nf = g.nfreq;
+  const int node = nodes[blockIdx.x];
+  const int lvl = depth[node] + g.rootlvl;
+  twiddles(w, n);
+  const T* den = supeden + (size_t)node * g.nsurf * g.sd;
+  for (int s = 0; s < g.sd; s++) {
+    T scale = (T)ldexp(1.0, lvl * g.deg[s]);  // plnden2effden scaling, matmgnt3d.cpp:228-235
+    for (int e = threadIdx.x; e < np * np * np; e += blockDim.x) xg[e] = T(0);
+    __syncthreads();
+    for (int k = threadIdx.x; k < g.nsurf; k += blockDim.x) {
+      int i = g.surf_ijk[3 * k], j = g.surf_ijk[3 * k + 1], kk = g.surf_ijk[3 * k + 2];
+      xg[(i * np + j) * np + kk] = den[(size_t)k * g.sd + s] * scale;
+    }
+    __syncthreads();
+    // x pass: A[k][j][kx] = sum_i x[i][j][k] w^(i kx)
+    for (int e = threadIdx.x; e < np * np * nh; e += blockDim.x) {
+      int kx = e % nh, j = (e / nh) % np, k = e / (nh * np);
+      T re = 0, im = 0;
+      for (int i = 0; i < np; i++) {
+        T v = xg[(i * np + j) * np + k];
+        Cpx<T> t = w[(i * kx) % n];
+        re += v * t.re;
+        im += v * t.im;
+      }
+      A[e].re = re;
+      A[e].im = im;
+    }
+    __syncthreads();
+    // y pass: B[k][ky][kx] = sum_j A[k][j][kx] w^(j ky)
+    for (int e = threadIdx.x; e < np * n * nh; e += blockDim.x) {
+      int kx = e % nh, ky = (e / nh) % n, k = e / (nh * n);
+      T re = 0, im = 0;
+      for (int j = 0; j < np; j++) {
+        Cpx<T> a = A[(k * np + j) * nh + kx];
+        Cpx<T> t = w[(j * ky) % n];
+        re += a.re * t.re - a.im * t.im;
+        im += a.re * t.im + a.im * t.re;
+      }
+      Bm[e].re = re;
+      Bm[e].im = im;
+    }
+    __syncthreads();
+    // z pass: out[kz][ky][kx] = sum_k B[k][ky][kx] w^(k kz)
+    T* out = spectra + ((size_t)node * g.sd + s) * nf * 2;
+    for (int e = threadIdx.x; e < nf; e += blockDim.x) {
+      int kxy = e % (n * nh), kz = e / (n * nh);
+      T re = 0, im = 0;
+      for (int k = 0; k < np; k++) {
+        Cpx<T> b = Bm[k * n * nh + kxy];
+        Cpx<T> t = w[(k * kz) % n];
+        re += b.re * t.re - b.im * t.im;
+        im += b.re * t.im + b.im * t.re;
+      }
+      out[2 * e] = re;
+      out[2 * e + 1] = im;
+    }
+    __syncthreads();
+  }
+}
+
+// effval[w][t][f] = sum_{s in V} sum_sd Khat[off][t][sd][f] * X[s][sd][f]   (cptwvv, matmgnt3d.cpp:343-360)
+template <typename T, int SD, int TD>
+__global__ void __launch_bounds__(FFT_THREADS) k_m2l_had(M2LGeom g, const T* __restrict__ khat,
+                                                          const T* __restrict__ spectra, const int* __restrict__ work,
+                                                          const int64_t* __restrict__ vptr,
+                                                          const int* __restrict__ vidx, const int* __restrict__ path,
+                                                          T* __restrict__ effval) {
+  // A V list holds at most 6^3 - 3^3 = 189 nodes (fmm3d/let3d.cpp:228-247);
+  // the host checks this bound before launching.
+  constexpr int VMAX = 192;
+  __shared__ int vs[VMAX], vo[VMAX];
+  const int wi = blockIdx.x;
+  const int t = work[wi];
+  const int nf = g.nfreq;
+  const int64_t b = vptr[wi];
+  const int cnt = (int)(vptr[wi + 1] - b);
+  const int tp0 = path[3 * t], tp1 = path[3 * t + 1], tp2 = path[3 * t + 2];
+  T* out = effval + (size_t)t * TD * nf * 2;
+  for (int q = threadIdx.x; q < cnt; q += blockDim.x) {
+    int s = vidx[b + q];
+    vs[q] = s;
+    vo[q] = (path[3 * s] - tp0 + 3) * 49 + (path[3 * s + 1] - tp1 + 3) * 7 + (path[3 * s + 2] - tp2 + 3);
+  }
+  __syncthreads();
+  for (int f = threadIdx.x; f < nf; f += blockDim.x) {
+    T ar[TD], ai[TD];
+#pragma unroll
+    for (int d = 0; d < TD; d++) ar[d] = ai[d] = T(0);
+    {
+      for (int q = 0; q < cnt; q++) {
+        const T* X = spectra + (size_t)vs[q] * SD * nf * 2;
+        const T* K = khat + (size_t)vo[q] * TD * SD * nf * 2;
+        T xr[SD], xi[SD];
+#pragma unroll
+        for (int s = 0; s < SD; s++) {
+          xr[s] = X[((size_t)s * nf + f) * 2];
+          xi[s] = X[((size_t)s * nf + f) * 2 + 1];
+        }
+#pragma unroll
+        for (int d = 0; d < TD; d++)
+#pragma unroll
+          for (int s = 0; s < SD; s++) {
+            T kr = K[(((size_t)d * SD + s) * nf + f) * 2];
+            T ki = K[(((size_t)d * SD + s) * nf + f) * 2 + 1];
+            ar[d] += kr * xr[s] - ki * xi[s];
+            ai[d] += kr * xi[s] + ki * xr[s];
+          }
+      }
+    }
+#pragma unroll
+    for (int d = 0; d < TD; d++) {
+      out[((size_t)d * nf + f) * 2] = ar[d];
+      out[((size_t)d * nf + f) * 2 + 1] = ai[d];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Hadamard accumulation in parent-pair form (single-dof equivalent kernel).
+//
+// The V list of a node t is the set of children c of the 26 colleagues P of
+// t's parent Q that are not adjacent to t (fmm3d/let3d.cpp:228-247), and the
+// translation from c to t depends only on the offset 2*(P-Q) + oct(c) -
+// oct(t), one of 316 values.  So per frequency the whole pass is, for every
+// target parent Q, Y[Q's 8 children] += sum_dir M_dir * X[P_dir's 8 children]
+// with 8x8 blocks drawn from the same 316 operator values.
+//
+// One CTA owns a tile of 32 frequencies (one per lane) for a slice of the
+// target parents; the 316 operator spectra of that tile sit in shared memory
+// for the CTA's whole lifetime.  A warp accumulates the 8 children of QPT
+// parents at once in registers, so each operator value read from shared
+// memory feeds QPT complex multiply-adds and each source spectrum read from
+// global memory feeds up to 8.
+__constant__ short c_pair_off[26 * 64];  // [dir][i][j] -> compact offset index, -1 when adjacent
+
+template <typename T, int QPT>
+__global__ void __launch_bounds__(256) k_m2l_had_pairs(int nf, const T* __restrict__ khat_c,
+                                                       const T* __restrict__ spectra, int nq,
+                                                       const int* __restrict__ qchd, const int* __restrict__ coll,
+                                                       const unsigned char* __restrict__ mask,
+                                                       T* __restrict__ effval) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Cpx<T>* Ks = reinterpret_cast<Cpx<T>*>(smem_raw);  // [316][32]
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int f0 = blockIdx.x * 32;
+  const int f = f0 + lane;
+  const bool fv = f < nf;
+  for (int e = threadIdx.x; e < 316 * 32; e += blockDim.x) {
+    int o = e >> 5, l = e & 31;
+    Cpx<T> v;
+    v.re = v.im = T(0);
+    if (f0 + l < nf) {
+      v.re = khat_c[((size_t)o * nf + f0 + l) * 2];
+      v.im = khat_c[((size_t)o * nf + f0 + l) * 2 + 1];
+    }
+    Ks[e] = v;
+  }
+  __syncthreads();
+  const int nwarps_total = gridDim.y * (blockDim.x >> 5);
+  const int gw = blockIdx.y * (blockDim.x >> 5) + warp;
+  for (int q0 = gw * QPT; q0 < nq; q0 += nwarps_total * QPT) {
+    T ar[QPT][8], ai[QPT][8];
+#pragma unroll
+    for (int q = 0; q < QPT; q++)
+#pragma unroll
+      for (int i = 0; i < 8; i++) ar[q][i] = ai[q][i] = T(0);
+    for (int dir = 0; dir < 26; dir++) {
+      int base[QPT];
+      bool any = false;
+#pragma unroll
+      for (int q = 0; q < QPT; q++) {
+        base[q] = (q0 + q < nq) ? coll[(size_t)(q0 + q) * 26 + dir] : -1;
+        any |= base[q] >= 0;
+      }
+      if (!any) continue;
+      const short* offs = &c_pair_off[dir * 64];
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        T xr[QPT], xi[QPT];
+#pragma unroll
+        for (int q = 0; q < QPT; q++) {
+          xr[q] = xi[q] = T(0);
+          if (base[q] >= 0 && fv) {
+            const T* X = spectra + ((size_t)(base[q] + j) * nf + f) * 2;
+            xr[q] = X[0];
+            xi[q] = X[1];
+          }
+        }
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+          int o = offs[i * 8 + j];
+          if (o < 0) continue;
+          Cpx<T> k = Ks[o * 32 + lane];
+#pragma unroll
+          for (int q = 0; q < QPT; q++) {
+            ar[q][i] += k.re * xr[q] - k.im * xi[q];
+            ai[q][i] += k.re * xi[q] + k.im * xr[q];
+          }
+        }
+      }
+    }
+    if (fv) {
+#pragma unroll
+      for (int q = 0; q < QPT; q++) {
+        if (q0 + q >= nq) continue;
+        int c0 = qchd[q0 + q];
+        unsigned m = mask[q0 + q];
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+          if (!((m >> i) & 1)) continue;
+          T* Y = effval + ((size_t)(c0 + i) * nf + f) * 2;
+          Y[0] = ar[q][i];
+          Y[1] = ai[q][i];
+        }
+      }
+    }
+  }
+}
+
+// tdncval[node][m][t] += real inverse transform of effval at the surface points
+template <typename T>
+__global__ void __launch_bounds__(FFT_THREADS) k_m2l_inv(M2LGeom g, const T* __restrict__ effval,
+                                                          const int* __restrict__ work, T* __restrict__ tdncval) {
+  // dynamic shared memory: Y[n*n*nh] | B[np*n*nh] | A[np*np*nh] | w[n]
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int np = g.np, n = g.n, nh = g.nh, nf = g.nfreq;
+  Cpx<T>* Y = reinterpret_cast<Cpx<T>*>(smem_raw);
+  Cpx<T>* Bm = Y + n * n * nh;
+  Cpx<T>* A = Bm + np * n * nh;
+  Cpx<T>* w = A + np * np * nh;
+  const int wi = blockIdx.x;
+  const int node = work[wi];
+  twiddles(w, n);
+  for (int t = 0; t < g.td; t++) {
+    const T* src = effval + ((size_t)node * g.td + t) * nf * 2;
+    for (int e = threadIdx.x; e < nf; e += blockDim.x) {
+      Y[e].re = src[2 * e];
+      Y[e].im = src[2 * e + 1];
+    }
+    __syncthreads();
+    // z pass (inverse): B[k][ky][kx] = sum_kz Y[kz][ky][kx] conj(w)^(k kz), k < np
+    for (int e = threadIdx.x; e < np * n * nh; e += blockDim.x) {
+      int kxy = e % (n * nh), k = e / (n * nh);
+      T re = 0, im = 0;
+      for (int kz = 0; kz < n; kz++) {
+        Cpx<T> y = Y[kz * n * nh + kxy];
+        Cpx<T> c = w[(k * kz) % n];
+        re += y.re * c.re + y.im * c.im;
+        im += y.im * c.re - y.re * c.im;
+      }
+      Bm[e].re = re;
+      Bm[e].im = im;
+    }
+    __syncthreads();
+    // y pass (inverse): A[k][j][kx] = sum_ky B[k][ky][kx] conj(w)^(j ky), j < np
+    for (int e = threadIdx.x; e < np * np * nh; e += blockDim.x) {
+      int kx = e % nh, j = (e / nh) % np, k = e / (nh * np);
+      T re = 0, im = 0;
+      for (int ky = 0; ky < n; ky++) {
+        Cpx<T> b = Bm[(k * n + ky) * nh + kx];
+        Cpx<T> c = w[(j * ky) % n];
+        re += b.re * c.re + b.im * c.im;
+        im += b.im * c.re - b.re * c.im;
+      }
+      A[e].re = re;
+      A[e].im = im;
+    }
+    __syncthreads();
+    // x pass (c2r, Hermitian half line) at the surface points only
+    T* dst = tdncval + (size_t)node * g.nsurf * g.td;
+    for (int m = threadIdx.x; m < g.nsurf; m += blockDim.x) {
+      int i = g.surf_ijk[3 * m], j = g.surf_ijk[3 * m + 1], k = g.surf_ijk[3 * m + 2];
+      const Cpx<T>* a = &A[(k * np + j) * nh];
+      T v = a[0].re + ((i & 1) ? -a[nh - 1].re : a[nh - 1].re);
+      T acc = 0;
+      for (int kx = 1; kx < nh - 1; kx++) {
+        Cpx<T> c = w[(i * kx) % n];
+        acc += a[kx].re * c.re + a[kx].im * c.im;  // Re(a * conj(w)^(i kx))
+      }
+      dst[(size_t)m * g.td + t] += v + T(2) * acc;
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace
+
+template <typename T>
+void launch_m2l_forward(const M2LGeom& g, const T* supeden, const int* nodes, int nn, const int* depth, T* spectra,
+                        cudaStream_t st) {
+  if (nn <= 0) return;
+  k_m2l_fwd<T><<<nn, FFT_THREADS, 0, st>>>(g, supeden, nodes, depth, spectra);
+}
+
+template <typename T>
+void launch_m2l_hadamard(const M2LGeom& g, const T* khat, const T* spectra, const int* work, int nwork,
+                         const int64_t* vptr, const int* vidx, const int* path, T* effval, cudaStream_t st) {
+  if (nwork <= 0) return;
+  if (g.sd == 1 && g.td == 1)
+    k_m2l_had<T, 1, 1><<<nwork, FFT_THREADS, 0, st>>>(g, khat, spectra, work, vptr, vidx, path, effval);
+  else if (g.sd == 4 && g.td == 3)
+    k_m2l_had<T, 4, 3><<<nwork, FFT_THREADS, 0, st>>>(g, khat, spectra, work, vptr, vidx, path, effval);
+  else if (g.sd == 3 && g.td == 3)
+    k_m2l_had<T, 3, 3><<<nwork, FFT_THREADS, 0, st>>>(g, khat, spectra, work, vptr, vidx, path, effval);
+}
+
+template <typename T>
+void launch_m2l_inverse(const M2LGeom& g, const T* effval, const int* work, int nwork, T* tdncval, cudaStream_t st) {
+  if (nwork <= 0) return;
+  size_t smem = sizeof(Cpx<T>) * ((size_t)g.n * g.n * g.nh + (size_t)g.np * g.n * g.nh + (size_t)g.np * g.np * g.nh + g.n);
+  if (smem > 48 * 1024) cudaFuncSetAttribute(k_m2l_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_m2l_inv<T><<<nwork, FFT_THREADS, smem, st>>>(g, effval, work, tdncval);
+}
+
+template <typename T>
+void launch_m2l_hadamard_pairs(int nf, const T* khat_c, const T* spectra, int nq, const int* qchd, const int* coll,
+                               const unsigned char* mask, T* effval, int num_sms, cudaStream_t st) {
+  if (nq <= 0) return;
+  constexpr int QPT = sizeof(T) == 4 ? 4 : 2;
+  size_t smem = sizeof(Cpx<T>) * 316 * 32;
+  cudaFuncSetAttribute(k_m2l_had_pairs<T, QPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int ftiles = (nf + 31) / 32;
+  int per_sm = sizeof(T) == 4 ? 2 : 1;
+  int qchunks = std::max(1, (num_sms * per_sm + ftiles - 1) / ftiles);
+  int warps_needed = (nq + QPT - 1) / QPT;
+  qchunks = std::min(qchunks, std::max(1, (warps_needed + 7) / 8));
+  dim3 grid(ftiles, qchunks);
+  k_m2l_had_pairs<T, QPT><<<grid, 256, smem, st>>>(nf, khat_c, spectra, nq, qchd, coll, mask, effval);
+}
+
+void m2l_set_pair_table(const short* tab, cudaStream_t st) {
+  cudaMemcpyToSymbolAsync(c_pair_off, tab, sizeof(short) * 26 * 64, 0, cudaMemcpyHostToDevice, st);
+}
+
+#define KIFMM_INST(T)                                                                                             \
+  template void launch_m2l_hadamard_pairs<T>(int, const T*, const T*, int, const int*, const int*,               \
+                                             const unsigned char*, T*, int, cudaStream_t);                         \
+  template void launch_m2l_forward<T>(const M2LGeom&, const T*, const int*, int, const int*, T*, cudaStream_t);  \
+  template void launch_m2l_hadamard<T>(const M2LGeom&, const T*, const T*, const int*, int, const int64_t*,     \
+                                       const int*, const int*, T*, cudaStream_t);                                \
+  template void launch_m2l_inverse<T>(const M2LGeom&, const T*, const int*, int, T*, cudaStream_t);
+KIFMM_INST(double)
+KIFMM_INST(float)
+#undef KIFMM_INST
+
+}  // namespace kifmm

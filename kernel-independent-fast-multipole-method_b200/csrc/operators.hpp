@@ -1,0 +1,75 @@
+// Translation operators of the KIFMM (host FP64 precompute, once per
+// (equivalent kernel, np), cached process-wide like the reference's
+// MatMgnt3d::getmmptr cache, fmm3d/matmgnt3d.cpp:438-452).
+//
+//   surface grids      MatMgnt3d::splposcal, fmm3d/matmgnt3d.cpp:375-398
+//   UC2UE, DC2DE       pseudo-inverses, fmm3d/matmgnt3d.cpp:91-123,158-188
+//   UE2UC, DE2DC       child/parent matrices, fmm3d/matmgnt3d.cpp:125-156,190-221
+//   M2L spectra        FFT of the kernel sampled on the (2np)^3 grid,
+//                      fmm3d/matmgnt3d.cpp:296-361 (regposcal :400-420)
+//
+// The device passes use fused forms: M2M = UC2UE * [UE2UC_0 .. UE2UC_7] and
+// L2L = [DC2DE * DE2DC_0; ..; DC2DE * DE2DC_7]; the per-level homogeneous
+// scalings 2^(+-l*deg) (fmm3d/matmgnt3d.cpp:107-118,141-153) are applied in
+// the GEMM prologue/epilogue.
+#pragma once
+
+#include <complex>
+#include <memory>
+#include <string>
+#include <vector>
+
+namespace kifmm {
+
+// Kernel ids of fmm3d/kernel3d.hpp:29-53 handled by FMM3d::setup.
+struct KernelDesc {
+  int kt = 0;
+  int sd = 0, td = 0;
+  bool dl = false;  // double layer: needs source normals
+  double coefs[2] = {1.0, 0.25};
+};
+
+bool kernel_desc(int kt, const double* coefs, int ncoef, KernelDesc* out);
+// FMM3d::setup's choice of equivalent-density kernel, fmm3d/fmm3d_setup.cpp:41-54.
+bool equivalent_kernel(const KernelDesc& user, KernelDesc* mm);
+// Homogeneity degree per source dof, Kernel3d::homsdeg (fmm3d/kernel3d.cpp:103-112).
+void homogeneous_degrees(int kt_mm, std::vector<int>* deg);
+
+// Row-major (n_t*td) x (n_s*sd) kernel matrix, Kernel3d::kernel semantics
+// (fmm3d/kernel3d.cpp:116-414), including the r < 1e-8 cut-off.
+void kernel_matrix(const KernelDesc& k, int nt, const double* trg, int ns, const double* src, const double* nor,
+                   double* out);
+
+// Pseudo-inverse V S^-1 U^T with singular values below rel_cut * s_max
+// dropped (pinv + SVDRep::construct, common/vecmatop.cpp:124-159,
+// common/svdrep.cpp:31-74).  a is m x n row-major; out is n x m row-major.
+// Returns false if the one-sided Jacobi SVD did not converge.
+bool pseudo_inverse(int m, int n, const double* a, double rel_cut, double* out, int nthreads);
+
+struct Operators {
+  KernelDesc mm;
+  int np = 0;
+  int nsurf = 0;          // |UE| = |DE| = |DC| = np^3 - (np-2)^3
+  int nuc = 0;            // |UC| = (np+2)^3 - np^3
+  int n = 0, nh = 0;      // FFT grid 2np, halved axis n/2+1
+  int nfreq = 0;          // n*n*nh
+  std::vector<int> deg;   // per sd
+  std::vector<double> ue, uc, de, dc;   // unit grids (3 per point), radii 1, 3, 3, 1
+  std::vector<int> surf_ijk;            // (i,j,k) grid index of each np-surface point
+  std::vector<double> uc2ue;            // (nsurf*sd) x (nuc*td)
+  std::vector<double> m2m;              // (nsurf*sd) x (8*nsurf*sd)
+  std::vector<double> dc2de;            // (nsurf*sd) x (nsurf*td)
+  std::vector<double> l2l;              // (8*nsurf*sd) x (nsurf*sd)
+  std::vector<std::complex<double>> m2l;  // [343 offsets][td][sd][nfreq], scaled by 1/n^3
+};
+
+// Builds (or returns the cached) operators; nullptr + err on failure.
+std::shared_ptr<const Operators> get_operators(const KernelDesc& mm, int np, int nthreads, std::string* err);
+
+// Surface grid of MatMgnt3d::splposcal(np, R): the np^3 lattice on [-R,R]^3
+// restricted to its boundary, x outermost and z innermost.
+void surface_grid(int np, double R, std::vector<double>* pos, std::vector<int>* ijk);
+
+inline int offset_index(int dx, int dy, int dz) { return (dx + 3) * 49 + (dy + 3) * 7 + (dz + 3); }
+
+}  // namespace kifmm

@@ -1,0 +1,395 @@
+// Point <-> point and point <-> surface evaluation passes.
+//
+//   k_s2m   S2M  : leaf sources -> its upward check surface      (SE2UC_dgemv, fmm3d/fmm3d.cpp:62-71)
+//   k_s2l   S2L  : X-list leaf sources -> downward check surface  (SE2DC_dgemv, fmm3d/fmm3d.cpp:73-82)
+//   k_leaf  near : U list + direct W/X (SE2TC_dgemv, fmm3d/fmm3d.cpp:35-60), M2T from W-list
+//                  upward equivalent surfaces (UE2TC_dgemv, :114-141) and L2T from the leaf's own
+//                  downward equivalent surface (DE2TC_dgemv, :84-112), fused into one pass that
+//                  writes each target once.
+//   k_direct     : FP64 direct sum (Dense3d::eval, fmm3d/dense3d.cpp:38-57).
+//
+// One CTA per work node.  Sources are staged through shared memory in tiles
+// and every target accumulates in registers; when a node has few targets the
+// CTA's threads split the source tile among several groups per target and
+// reduce through shared memory at the end.  Positions are stored relative to
+// the centre of their leaf and re-centred on the target node's centre while
+// staging, so FP32 differences lose no more than the node size's precision.
+#include "kernels_common.cuh"
+#include "launch.hpp"
+
+namespace kifmm {
+
+namespace {
+
+constexpr int P2P_THREADS = 128;
+constexpr int TILE = 256;
+
+template <typename T, int SDMAX>
+struct Tile {
+  T x[TILE], y[TILE], z[TILE];
+  T nx[TILE], ny[TILE], nz[TILE];
+  T f[TILE * SDMAX];
+};
+
+template <typename T, int TDMAX>
+struct Red {
+  T v[P2P_THREADS * TDMAX];
+};
+
+__device__ __forceinline__ int group_size(int nt) {
+  int g = ((nt + 31) / 32) * 32;
+  return g > P2P_THREADS ? P2P_THREADS : (g < 32 ? 32 : g);
+}
+
+// Stages points [b, b+cnt) of a source leaf (local coords + shift) into the tile.
+template <typename T, int SD, bool DL>
+__device__ __forceinline__ void stage_points(Tile<T, 4>& t, const P2PArgs<T>& a, int b, int cnt, T shx, T shy,
+                                             T shz, int rhs) {
+  for (int j = threadIdx.x; j < cnt; j += blockDim.x) {
+    int p = b + j;
+    t.x[j] = a.sx[p] + shx;
+    t.y[j] = a.sy[p] + shy;
+    t.z[j] = a.sz[p] + shz;
+    if constexpr (DL) {
+      t.nx[j] = a.snx[p];
+      t.ny[j] = a.sny[p];
+      t.nz[j] = a.snz[p];
+    }
+#pragma unroll
+    for (int s = 0; s < SD; s++) t.f[j * SD + s] = a.sden[(size_t)rhs * a.ns * SD + (size_t)p * SD + s];
+  }
+}
+
+// Stages `cnt` points of a surface grid (unit * rad + shift) with densities den[k*SD + s].
+template <typename T, int SD>
+__device__ __forceinline__ void stage_surface(Tile<T, 4>& t, const T* unit, int k0, int cnt, T rad, T shx, T shy,
+                                              T shz, const T* den) {
+  for (int j = threadIdx.x; j < cnt; j += blockDim.x) {
+    int k = k0 + j;
+    t.x[j] = unit[3 * k] * rad + shx;
+    t.y[j] = unit[3 * k + 1] * rad + shy;
+    t.z[j] = unit[3 * k + 2] * rad + shz;
+#pragma unroll
+    for (int s = 0; s < SD; s++) t.f[j * SD + s] = den[(size_t)k * SD + s];
+  }
+}
+
+template <typename T, int KT>
+__device__ __forceinline__ void accumulate_tile(const Tile<T, 4>& t, int cnt, int j0, int jstep, T px, T py, T pz,
+                                                T* acc, const KConst<T>& kc) {
+  constexpr int SD = KTraits<KT>::SD;
+  for (int j = j0; j < cnt; j += jstep) {
+    T nrm[3];
+    if constexpr (KTraits<KT>::DL) {
+      nrm[0] = t.nx[j];
+      nrm[1] = t.ny[j];
+      nrm[2] = t.nz[j];
+    }
+    keval<KT, T>(px - t.x[j], py - t.y[j], pz - t.z[j], nrm, &t.f[j * SD], acc, kc);
+  }
+}
+
+template <typename T, int TD>
+__device__ __forceinline__ void reduce_and_store(Red<T, 4>& red, const T* acc, int G, int nsplit, bool valid,
+                                                 T* out, bool add) {
+  int slot = threadIdx.x % G, sg = threadIdx.x / G;
+  if (sg < nsplit) {
+#pragma unroll
+    for (int d = 0; d < TD; d++) red.v[(sg * G + slot) * TD + d] = acc[d];
+  }
+  __syncthreads();
+  if (sg == 0 && valid) {
+#pragma unroll
+    for (int d = 0; d < TD; d++) {
+      T s = red.v[slot * TD + d];
+      for (int q = 1; q < nsplit; q++) s += red.v[(q * G + slot) * TD + d];
+      if (add)
+        out[d] += s;
+      else
+        out[d] = s;
+    }
+  }
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+template <typename T, int KT>
+__global__ void __launch_bounds__(P2P_THREADS) k_s2m(P2PArgs<T> a, const int* work, int nwork, int rhs) {
+  constexpr int SD = KTraits<KT>::SD, TD = KTraits<KT>::TD;
+  constexpr bool DL = KTraits<KT>::DL;
+  __shared__ Tile<T, 4> tile;
+  __shared__ Red<T, 4> red;
+  int g = work[blockIdx.x];
+  T rad = (T)a.radius[g];
+  int nt = a.nuc;
+  int G = group_size(nt), nsplit = P2P_THREADS / G;
+  int slot = threadIdx.x % G, sg = threadIdx.x / G;
+  int sb = a.sbeg[g], sc = a.scnt[g];
+  T* outbase = a.supcval + (size_t)g * a.nuc * TD;
+  for (int tb = 0; tb < nt; tb += G) {
+    int ti = tb + slot;
+    bool valid = ti < nt && sg < nsplit;
+    T px = 0, py = 0, pz = 0;
+    if (valid) {
+      px = a.uc_unit[3 * ti] * rad;
+      py = a.uc_unit[3 * ti + 1] * rad;
+      pz = a.uc_unit[3 * ti + 2] * rad;
+    }
+    T acc[4] = {0, 0, 0, 0};
+    for (int c0 = 0; c0 < sc; c0 += TILE) {
+      int cnt = min(TILE, sc - c0);
+      __syncthreads();
+      stage_points<T, SD, DL>(tile, a, sb + c0, cnt, T(0), T(0), T(0), rhs);
+      __syncthreads();
+      if (valid) accumulate_tile<T, KT>(tile, cnt, sg, nsplit, px, py, pz, acc, a.ku);
+    }
+    reduce_and_store<T, TD>(red, acc, G, nsplit, ti < nt, outbase + (size_t)ti * TD, false);
+  }
+}
+
+template <typename T, int KT>
+__global__ void __launch_bounds__(P2P_THREADS) k_s2l(P2PArgs<T> a, const int* work, const int64_t* ptr,
+                                                      const int* idx, int nwork, int rhs) {
+  constexpr int SD = KTraits<KT>::SD, TD = KTraits<KT>::TD;
+  constexpr bool DL = KTraits<KT>::DL;
+  __shared__ Tile<T, 4> tile;
+  __shared__ Red<T, 4> red;
+  int w = blockIdx.x;
+  int g = work[w];
+  T rad = (T)a.radius[g];
+  double cx = a.center[3 * g], cy = a.center[3 * g + 1], cz = a.center[3 * g + 2];
+  int nt = a.nsurf;
+  int G = group_size(nt), nsplit = P2P_THREADS / G;
+  int slot = threadIdx.x % G, sg = threadIdx.x / G;
+  T* outbase = a.tdncval + (size_t)g * a.nsurf * TD;
+  for (int tb = 0; tb < nt; tb += G) {
+    int ti = tb + slot;
+    bool valid = ti < nt && sg < nsplit;
+    T px = 0, py = 0, pz = 0;
+    if (valid) {
+      px = a.dc_unit[3 * ti] * rad;
+      py = a.dc_unit[3 * ti + 1] * rad;
+      pz = a.dc_unit[3 * ti + 2] * rad;
+    }
+    T acc[4] = {0, 0, 0, 0};
+    for (int64_t e = ptr[w]; e < ptr[w + 1]; e++) {
+      int s = idx[e];
+      T shx = (T)(a.center[3 * s] - cx), shy = (T)(a.center[3 * s + 1] - cy), shz = (T)(a.center[3 * s + 2] - cz);
+      int sb = a.sbeg[s], sc = a.scnt[s];
+      for (int c0 = 0; c0 < sc; c0 += TILE) {
+        int cnt = min(TILE, sc - c0);
+        __syncthreads();
+        stage_points<T, SD, DL>(tile, a, sb + c0, cnt, shx, shy, shz, rhs);
+        __syncthreads();
+        if (valid) accumulate_tile<T, KT>(tile, cnt, sg, nsplit, px, py, pz, acc, a.ku);
+      }
+    }
+    reduce_and_store<T, TD>(red, acc, G, nsplit, ti < nt, outbase + (size_t)ti * TD, true);
+  }
+}
+
+template <typename T, int KT>
+__global__ void __launch_bounds__(P2P_THREADS) k_leaf(P2PArgs<T> a, const int* work, const int64_t* nptr,
+                                                       const int* nidx, const int64_t* mptr, const int* midx,
+                                                       int nwork, int rhs) {
+  constexpr int SD = KTraits<KT>::SD, TD = KTraits<KT>::TD;
+  constexpr bool DL = KTraits<KT>::DL;
+  constexpr int MM = KTraits<KT>::MM;
+  constexpr int SDM = KTraits<MM>::SD;
+  __shared__ Tile<T, 4> tile;
+  __shared__ Red<T, 4> red;
+  int w = blockIdx.x;
+  int g = work[w];
+  double cx = a.center[3 * g], cy = a.center[3 * g + 1], cz = a.center[3 * g + 2];
+  T rad = (T)a.radius[g];
+  int tb0 = a.tbeg[g], nt = a.tcnt[g];
+  int G = group_size(nt), nsplit = P2P_THREADS / G;
+  int slot = threadIdx.x % G, sg = threadIdx.x / G;
+  bool l2t = a.depth[g] >= 2;
+  T* outbase = a.tval + (size_t)rhs * a.nt * TD;
+  const T* tdn = a.tdneden + (size_t)g * a.nsurf * SDM;
+  for (int tb = 0; tb < nt; tb += G) {
+    int ti = tb + slot;
+    bool valid = ti < nt && sg < nsplit;
+    T px = 0, py = 0, pz = 0;
+    if (valid) {
+      px = a.tx[tb0 + ti];
+      py = a.ty[tb0 + ti];
+      pz = a.tz[tb0 + ti];
+    }
+    T acc[4] = {0, 0, 0, 0};
+    // point sources: U list, direct W and X (user kernel, with normals)
+    for (int64_t e = nptr[w]; e < nptr[w + 1]; e++) {
+      int s = nidx[e];
+      T shx = (T)(a.center[3 * s] - cx), shy = (T)(a.center[3 * s + 1] - cy), shz = (T)(a.center[3 * s + 2] - cz);
+      int sb = a.sbeg[s], sc = a.scnt[s];
+      for (int c0 = 0; c0 < sc; c0 += TILE) {
+        int cnt = min(TILE, sc - c0);
+        __syncthreads();
+        stage_points<T, SD, DL>(tile, a, sb + c0, cnt, shx, shy, shz, rhs);
+        __syncthreads();
+        if (valid) accumulate_tile<T, KT>(tile, cnt, sg, nsplit, px, py, pz, acc, a.ku);
+      }
+    }
+    // M2T: W-list upward equivalent surfaces (equivalent kernel)
+    for (int64_t e = mptr[w]; e < mptr[w + 1]; e++) {
+      int s = midx[e];
+      T shx = (T)(a.center[3 * s] - cx), shy = (T)(a.center[3 * s + 1] - cy), shz = (T)(a.center[3 * s + 2] - cz);
+      const T* den = a.supeden + (size_t)s * a.nsurf * SDM;
+      T rs = (T)a.radius[s];
+      for (int c0 = 0; c0 < a.nsurf; c0 += TILE) {
+        int cnt = min(TILE, a.nsurf - c0);
+        __syncthreads();
+        stage_surface<T, SDM>(tile, a.ue_unit, c0, cnt, rs, shx, shy, shz, den);
+        __syncthreads();
+        if (valid) accumulate_tile<T, MM>(tile, cnt, sg, nsplit, px, py, pz, acc, a.km);
+      }
+    }
+    // L2T: own downward equivalent surface
+    if (l2t) {
+      for (int c0 = 0; c0 < a.nsurf; c0 += TILE) {
+        int cnt = min(TILE, a.nsurf - c0);
+        __syncthreads();
+        stage_surface<T, SDM>(tile, a.de_unit, c0, cnt, rad, T(0), T(0), T(0), tdn);
+        __syncthreads();
+        if (valid) accumulate_tile<T, MM>(tile, cnt, sg, nsplit, px, py, pz, acc, a.km);
+      }
+    }
+    reduce_and_store<T, TD>(red, acc, G, nsplit, ti < nt, outbase + (size_t)(tb0 + ti) * TD, false);
+  }
+}
+
+// FP64 direct sum over all sources, absolute coordinates (3 x n interleaved).
+template <int KT>
+__global__ void __launch_bounds__(P2P_THREADS) k_direct(const double* spos, const double* snor, const double* sden,
+                                                         int ns, const double* tpos, int nt, double* out,
+                                                         KConst<double> kc) {
+  constexpr int SD = KTraits<KT>::SD, TD = KTraits<KT>::TD;
+  __shared__ double sx[TILE], sy[TILE], sz[TILE], nx[TILE], ny[TILE], nz[TILE], f[TILE * 4];
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  double px = 0, py = 0, pz = 0;
+  if (t < nt) {
+    px = tpos[3 * t];
+    py = tpos[3 * t + 1];
+    pz = tpos[3 * t + 2];
+  }
+  double acc[4] = {0, 0, 0, 0};
+  for (int c0 = 0; c0 < ns; c0 += TILE) {
+    int cnt = min(TILE, ns - c0);
+    __syncthreads();
+    for (int j = threadIdx.x; j < cnt; j += blockDim.x) {
+      int p = c0 + j;
+      sx[j] = spos[3 * p];
+      sy[j] = spos[3 * p + 1];
+      sz[j] = spos[3 * p + 2];
+      nx[j] = snor[3 * p];
+      ny[j] = snor[3 * p + 1];
+      nz[j] = snor[3 * p + 2];
+      for (int s = 0; s < SD; s++) f[j * SD + s] = sden[(size_t)p * SD + s];
+    }
+    __syncthreads();
+    if (t < nt)
+      for (int j = 0; j < cnt; j++) {
+        double nrm[3] = {nx[j], ny[j], nz[j]};
+        keval<KT, double>(px - sx[j], py - sy[j], pz - sz[j], nrm, &f[j * SD], acc, kc);
+      }
+  }
+  if (t < nt)
+    for (int d = 0; d < TD; d++) out[(size_t)t * TD + d] = acc[d];
+}
+
+// sden_sorted[r][i][s] = srcden[r][perm[i]][s]
+template <typename T>
+__global__ void k_scatter_den(const double* srcden, const int* perm, int ns, int sd, int nrhs, T* out) {
+  size_t n = (size_t)ns * sd * nrhs;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    size_t r = e / ((size_t)ns * sd);
+    size_t rem = e % ((size_t)ns * sd);
+    int i = (int)(rem / sd), s = (int)(rem % sd);
+    out[e] = (T)srcden[r * ns * sd + (size_t)perm[i] * sd + s];
+  }
+}
+
+// trgval[r][perm[i]][t] = tval[r][i][t]
+template <typename T>
+__global__ void k_gather_val(const T* tval, const int* perm, int nt, int td, int nrhs, double* trgval) {
+  size_t n = (size_t)nt * td * nrhs;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    size_t r = e / ((size_t)nt * td);
+    size_t rem = e % ((size_t)nt * td);
+    int i = (int)(rem / td), d = (int)(rem % td);
+    trgval[r * nt * td + (size_t)perm[i] * td + d] = (double)tval[e];
+  }
+}
+
+template <typename T, int KT>
+void launch_p2p_kt(const P2PArgs<T>& a, const P2PWork& w, int which, int rhs, cudaStream_t st) {
+  switch (which) {
+    case P2P_S2M:
+      if (w.n) k_s2m<T, KT><<<w.n, P2P_THREADS, 0, st>>>(a, w.work, w.n, rhs);
+      break;
+    case P2P_S2L:
+      if (w.n) k_s2l<T, KT><<<w.n, P2P_THREADS, 0, st>>>(a, w.work, w.ptr, w.idx, w.n, rhs);
+      break;
+    case P2P_LEAF:
+      if (w.n) k_leaf<T, KT><<<w.n, P2P_THREADS, 0, st>>>(a, w.work, w.ptr, w.idx, w.ptr2, w.idx2, w.n, rhs);
+      break;
+  }
+}
+
+}  // namespace
+
+template <typename T>
+void launch_p2p(int kt, const P2PArgs<T>& a, const P2PWork& w, int which, int rhs, cudaStream_t st) {
+  switch (kt) {
+    case 111: launch_p2p_kt<T, 111>(a, w, which, rhs, st); break;
+    case 121: launch_p2p_kt<T, 121>(a, w, which, rhs, st); break;
+    case 311: launch_p2p_kt<T, 311>(a, w, which, rhs, st); break;
+    case 312: launch_p2p_kt<T, 312>(a, w, which, rhs, st); break;
+    case 321: launch_p2p_kt<T, 321>(a, w, which, rhs, st); break;
+    case 322: launch_p2p_kt<T, 322>(a, w, which, rhs, st); break;
+    case 511: launch_p2p_kt<T, 511>(a, w, which, rhs, st); break;
+    case 521: launch_p2p_kt<T, 521>(a, w, which, rhs, st); break;
+  }
+}
+template void launch_p2p<double>(int, const P2PArgs<double>&, const P2PWork&, int, int, cudaStream_t);
+template void launch_p2p<float>(int, const P2PArgs<float>&, const P2PWork&, int, int, cudaStream_t);
+
+void launch_direct(int kt, const double* spos, const double* snor, const double* sden, int ns, const double* tpos,
+                   int nt, double* out, const double* kc3, cudaStream_t st) {
+  KConst<double> kc{kc3[0], kc3[1], kc3[2]};
+  int grid = (nt + P2P_THREADS - 1) / P2P_THREADS;
+  if (grid == 0) return;
+  switch (kt) {
+    case 111: k_direct<111><<<grid, P2P_THREADS, 0, st>>>(spos, snor, sden, ns, tpos, nt, out, kc); break;
+    case 121: k_direct<121><<<grid, P2P_THREADS, 0, st>>>(spos, snor, sden, ns, tpos, nt, out, kc); break;
+    case 311: k_direct<311><<<grid, P2P_THREADS, 0, st>>>(spos, snor, sden, ns, tpos, nt, out, kc); break;
+    case 312: k_direct<312><<<grid, P2P_THREADS, 0, st>>>(spos, snor, sden, ns, tpos, nt, out, kc); break;
+    case 321: k_direct<321><<<grid, P2P_THREADS, 0, st>>>(spos, snor, sden, ns, tpos, nt, out, kc); break;
+    case 322: k_direct<322><<<grid, P2P_THREADS, 0, st>>>(spos, snor, sden, ns, tpos, nt, out, kc); break;
+    case 511: k_direct<511><<<grid, P2P_THREADS, 0, st>>>(spos, snor, sden, ns, tpos, nt, out, kc); break;
+    case 521: k_direct<521><<<grid, P2P_THREADS, 0, st>>>(spos, snor, sden, ns, tpos, nt, out, kc); break;
+  }
+}
+
+template <typename T>
+void launch_scatter_den(const double* srcden, const int* perm, int ns, int sd, int nrhs, T* out, cudaStream_t st) {
+  size_t n = (size_t)ns * sd * nrhs;
+  if (!n) return;
+  int grid = (int)std::min<size_t>((n + 255) / 256, 148 * 16);
+  k_scatter_den<T><<<grid, 256, 0, st>>>(srcden, perm, ns, sd, nrhs, out);
+}
+template void launch_scatter_den<double>(const double*, const int*, int, int, int, double*, cudaStream_t);
+template void launch_scatter_den<float>(const double*, const int*, int, int, int, float*, cudaStream_t);
+
+template <typename T>
+void launch_gather_val(const T* tval, const int* perm, int nt, int td, int nrhs, double* trgval, cudaStream_t st) {
+  size_t n = (size_t)nt * td * nrhs;
+  if (!n) return;
+  int grid = (int)std::min<size_t>((n + 255) / 256, 148 * 16);
+  k_gather_val<T><<<grid, 256, 0, st>>>(tval, perm, nt, td, nrhs, trgval);
+}
+template void launch_gather_val<double>(const double*, const int*, int, int, int, double*, cudaStream_t);
+template void launch_gather_val<float>(const float*, const int*, int, int, int, double*, cudaStream_t);
+
+}  // namespace kifmm
