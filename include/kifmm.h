@@ -85,8 +85,8 @@ kifmm_status kifmm_eval_multi(kifmm_handle h, int nrhs, const double* srcden, do
 
 /* Device-resident form: d_srcden / d_trgval are device pointers (double,
  * same layout as kifmm_eval_multi); the work is enqueued on `stream`
- * (a cudaStream_t, or NULL for the engine's own stream) and the call
- * returns without synchronising when sync == 0. */
+ * (a cudaStream_t; NULL is the legacy default stream, as everywhere in
+ * CUDA) and the call returns without synchronising when sync == 0. */
 kifmm_status kifmm_eval_device(kifmm_handle h, int nrhs, const double* d_srcden, double* d_trgval, void* stream,
                                int sync);
 

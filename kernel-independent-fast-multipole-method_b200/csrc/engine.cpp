@@ -691,9 +691,8 @@ int Engine::eval_device(const double* d_srcden, double* d_trgval, int nrhs, cuda
     err = "bad eval arguments";
     return KIFMM_ERR_ARG;
   }
-  if (!st) st = stream;
   try {
-    int rc = impl->eval(d_srcden, d_trgval, nrhs, st);
+    int rc = impl->eval(d_srcden, d_trgval, nrhs, st);  // st as given: NULL is the legacy default stream
     if (rc != KIFMM_OK) return rc;
     if (sync) KCHECK(cudaStreamSynchronize(st));
   } catch (const CudaError& e) {

@@ -188,6 +188,33 @@ __global__ void __launch_bounds__(P2P_THREADS) k_s2l(P2PArgs<T> a, const int* wo
   }
 }
 
+// Segment table of the sources a CTA stages: a run of point leaves or of
+// surface grids, flattened so that one shared-memory tile can span many
+// small segments (leaves average a dozen points at ptsmax=64, so staging one
+// leaf per barrier pair would leave the CTA mostly waiting).
+constexpr int SEGS = 64;
+
+template <typename T>
+struct Segs {
+  int beg[SEGS];        // first sorted point (point segments) or node id (surface segments)
+  int pre[SEGS + 1];    // prefix sums of the segment sizes
+  T shx[SEGS], shy[SEGS], shz[SEGS], rad[SEGS];
+  const T* unit[SEGS];  // surface grid (surface segments)
+  const T* den[SEGS];   // surface densities (surface segments)
+};
+
+__device__ __forceinline__ int find_seg(const int* pre, int ns, int k) {
+  int lo = 0, hi = ns;  // pre[lo] <= k < pre[hi]
+  while (hi - lo > 1) {
+    int mid = (lo + hi) >> 1;
+    if (pre[mid] <= k)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
 template <typename T, int KT>
 __global__ void __launch_bounds__(P2P_THREADS) k_leaf(P2PArgs<T> a, const int* work, const int64_t* nptr,
                                                        const int* nidx, const int64_t* mptr, const int* midx,
@@ -198,19 +225,24 @@ __global__ void __launch_bounds__(P2P_THREADS) k_leaf(P2PArgs<T> a, const int* w
   constexpr int SDM = KTraits<MM>::SD;
   __shared__ Tile<T, 4> tile;
   __shared__ Red<T, 4> red;
-  int w = blockIdx.x;
-  int g = work[w];
-  double cx = a.center[3 * g], cy = a.center[3 * g + 1], cz = a.center[3 * g + 2];
-  T rad = (T)a.radius[g];
-  int tb0 = a.tbeg[g], nt = a.tcnt[g];
-  int G = group_size(nt), nsplit = P2P_THREADS / G;
-  int slot = threadIdx.x % G, sg = threadIdx.x / G;
-  bool l2t = a.depth[g] >= 2;
+  __shared__ Segs<T> seg;
+  const int w = blockIdx.x;
+  const int g = work[w];
+  const double cx = a.center[3 * g], cy = a.center[3 * g + 1], cz = a.center[3 * g + 2];
+  const T rad = (T)a.radius[g];
+  const int tb0 = a.tbeg[g], nt = a.tcnt[g];
+  // thread -> (target slot, source split): every thread of the CTA is busy
+  const int G = nt < P2P_THREADS ? (nt > 0 ? nt : 1) : P2P_THREADS;
+  const int nsplit = P2P_THREADS / G;
+  const int slot = threadIdx.x % G, sg = threadIdx.x / G;
+  const bool l2t = a.depth[g] >= 2;
   T* outbase = a.tval + (size_t)rhs * a.nt * TD;
-  const T* tdn = a.tdneden + (size_t)g * a.nsurf * SDM;
+  const int64_t nb = nptr[w], ne = nptr[w + 1];
+  const int64_t mb = mptr[w], me = mptr[w + 1];
+  const int nsurf_segs = (int)(me - mb) + (l2t ? 1 : 0);
   for (int tb = 0; tb < nt; tb += G) {
-    int ti = tb + slot;
-    bool valid = ti < nt && sg < nsplit;
+    const int ti = tb + slot;
+    const bool valid = ti < nt && sg < nsplit;
     T px = 0, py = 0, pz = 0;
     if (valid) {
       px = a.tx[tb0 + ti];
@@ -219,40 +251,86 @@ __global__ void __launch_bounds__(P2P_THREADS) k_leaf(P2PArgs<T> a, const int* w
     }
     T acc[4] = {0, 0, 0, 0};
     // point sources: U list, direct W and X (user kernel, with normals)
-    for (int64_t e = nptr[w]; e < nptr[w + 1]; e++) {
-      int s = nidx[e];
-      T shx = (T)(a.center[3 * s] - cx), shy = (T)(a.center[3 * s + 1] - cy), shz = (T)(a.center[3 * s + 2] - cz);
-      int sb = a.sbeg[s], sc = a.scnt[s];
-      for (int c0 = 0; c0 < sc; c0 += TILE) {
-        int cnt = min(TILE, sc - c0);
-        __syncthreads();
-        stage_points<T, SD, DL>(tile, a, sb + c0, cnt, shx, shy, shz, rhs);
+    for (int64_t c0 = nb; c0 < ne; c0 += SEGS) {
+      const int nseg = (int)min((int64_t)SEGS, ne - c0);
+      __syncthreads();
+      if (threadIdx.x < nseg) {
+        int s = nidx[c0 + threadIdx.x];
+        seg.beg[threadIdx.x] = a.sbeg[s];
+        seg.pre[threadIdx.x + 1] = a.scnt[s];
+        seg.shx[threadIdx.x] = (T)(a.center[3 * s] - cx);
+        seg.shy[threadIdx.x] = (T)(a.center[3 * s + 1] - cy);
+        seg.shz[threadIdx.x] = (T)(a.center[3 * s + 2] - cz);
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        seg.pre[0] = 0;
+        for (int e = 0; e < nseg; e++) seg.pre[e + 1] += seg.pre[e];
+      }
+      __syncthreads();
+      const int total = seg.pre[nseg];
+      for (int k0 = 0; k0 < total; k0 += TILE) {
+        const int cnt = min(TILE, total - k0);
+        for (int j = threadIdx.x; j < cnt; j += blockDim.x) {
+          int k = k0 + j;
+          int e = find_seg(seg.pre, nseg, k);
+          int p = seg.beg[e] + (k - seg.pre[e]);
+          tile.x[j] = a.sx[p] + seg.shx[e];
+          tile.y[j] = a.sy[p] + seg.shy[e];
+          tile.z[j] = a.sz[p] + seg.shz[e];
+          if constexpr (DL) {
+            tile.nx[j] = a.snx[p];
+            tile.ny[j] = a.sny[p];
+            tile.nz[j] = a.snz[p];
+          }
+#pragma unroll
+          for (int s = 0; s < SD; s++) tile.f[j * SD + s] = a.sden[(size_t)rhs * a.ns * SD + (size_t)p * SD + s];
+        }
         __syncthreads();
         if (valid) accumulate_tile<T, KT>(tile, cnt, sg, nsplit, px, py, pz, acc, a.ku);
+        __syncthreads();
       }
     }
-    // M2T: W-list upward equivalent surfaces (equivalent kernel)
-    for (int64_t e = mptr[w]; e < mptr[w + 1]; e++) {
-      int s = midx[e];
-      T shx = (T)(a.center[3 * s] - cx), shy = (T)(a.center[3 * s + 1] - cy), shz = (T)(a.center[3 * s + 2] - cz);
-      const T* den = a.supeden + (size_t)s * a.nsurf * SDM;
-      T rs = (T)a.radius[s];
-      for (int c0 = 0; c0 < a.nsurf; c0 += TILE) {
-        int cnt = min(TILE, a.nsurf - c0);
-        __syncthreads();
-        stage_surface<T, SDM>(tile, a.ue_unit, c0, cnt, rs, shx, shy, shz, den);
-        __syncthreads();
-        if (valid) accumulate_tile<T, MM>(tile, cnt, sg, nsplit, px, py, pz, acc, a.km);
+    // surface sources: W-list upward equivalent surfaces (M2T) and the leaf's
+    // own downward equivalent surface (L2T), equivalent kernel
+    for (int c0 = 0; c0 < nsurf_segs; c0 += SEGS) {
+      const int nseg = min(SEGS, nsurf_segs - c0);
+      __syncthreads();
+      if (threadIdx.x < nseg) {
+        int e = c0 + threadIdx.x;
+        if (e < (int)(me - mb)) {
+          int s = midx[mb + e];
+          seg.shx[threadIdx.x] = (T)(a.center[3 * s] - cx);
+          seg.shy[threadIdx.x] = (T)(a.center[3 * s + 1] - cy);
+          seg.shz[threadIdx.x] = (T)(a.center[3 * s + 2] - cz);
+          seg.rad[threadIdx.x] = (T)a.radius[s];
+          seg.unit[threadIdx.x] = a.ue_unit;
+          seg.den[threadIdx.x] = a.supeden + (size_t)s * a.nsurf * SDM;
+        } else {
+          seg.shx[threadIdx.x] = seg.shy[threadIdx.x] = seg.shz[threadIdx.x] = T(0);
+          seg.rad[threadIdx.x] = rad;
+          seg.unit[threadIdx.x] = a.de_unit;
+          seg.den[threadIdx.x] = a.tdneden + (size_t)g * a.nsurf * SDM;
+        }
       }
-    }
-    // L2T: own downward equivalent surface
-    if (l2t) {
-      for (int c0 = 0; c0 < a.nsurf; c0 += TILE) {
-        int cnt = min(TILE, a.nsurf - c0);
-        __syncthreads();
-        stage_surface<T, SDM>(tile, a.de_unit, c0, cnt, rad, T(0), T(0), T(0), tdn);
+      __syncthreads();
+      const int total = nseg * a.nsurf;
+      for (int k0 = 0; k0 < total; k0 += TILE) {
+        const int cnt = min(TILE, total - k0);
+        for (int j = threadIdx.x; j < cnt; j += blockDim.x) {
+          int k = k0 + j;
+          int e = k / a.nsurf, m = k - e * a.nsurf;
+          const T* u = seg.unit[e];
+          T r = seg.rad[e];
+          tile.x[j] = u[3 * m] * r + seg.shx[e];
+          tile.y[j] = u[3 * m + 1] * r + seg.shy[e];
+          tile.z[j] = u[3 * m + 2] * r + seg.shz[e];
+#pragma unroll
+          for (int s = 0; s < SDM; s++) tile.f[j * SDM + s] = seg.den[e][(size_t)m * SDM + s];
+        }
         __syncthreads();
         if (valid) accumulate_tile<T, MM>(tile, cnt, sg, nsplit, px, py, pz, acc, a.km);
+        __syncthreads();
       }
     }
     reduce_and_store<T, TD>(red, acc, G, nsplit, ti < nt, outbase + (size_t)(tb0 + ti) * TD, false);

@@ -244,7 +244,7 @@ class FMM3d:
         self._check(lib().kifmm_set_profiling(self._h, 1 if on else 0))
 
     def phase_times(self):
-        ms = (ctypes.c_double * 8)()
+        ms = (ctypes.c_double * 16)()
         n = ctypes.c_int()
         self._check(lib().kifmm_phase_times(self._h, ms, ctypes.byref(n)))
         names = ("upward", "vlist", "xlist", "downward", "leaf", "total", "m2l_forward", "m2l_hadamard",

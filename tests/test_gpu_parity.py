@@ -128,10 +128,29 @@ def test_device_pointer_api(gpu):
     f.eval(d["den"], host)
     sden = torch.tensor(d["den"], device="cuda", dtype=torch.float64)
     tval = torch.zeros(len(d["trg"]), device="cuda", dtype=torch.float64)
-    st = torch.cuda.current_stream()
+    st = torch.cuda.current_stream()  # the legacy default stream: handle 0
     f.eval_device(sden.data_ptr(), tval.data_ptr(), 1, st.cuda_stream, sync=False)
-    st.synchronize()
-    assert np.array_equal(tval.cpu().numpy(), host)
+    assert np.array_equal(tval.cpu().numpy(), host)  # ordered on the caller's stream
+    side = torch.cuda.Stream()
+    tval2 = torch.zeros_like(tval)
+    torch.cuda.synchronize()
+    f.eval_device(sden.data_ptr(), tval2.data_ptr(), 1, side.cuda_stream, sync=False)
+    side.synchronize()
+    assert np.array_equal(tval2.cpu().numpy(), host)
+
+
+def test_reference_style_cli_driver(gpu):
+    import os
+    import re
+    import subprocess
+    pkg = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                       "kernel-independent-fast-multipole-method_b200")
+    exe = os.path.join(pkg, "lib", "tt_b200")
+    r = subprocess.run([exe, os.path.join(pkg, "examples", "options_laplace_np4.txt"), "3"], capture_output=True,
+                       text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    err = float(re.search(r"relative error ([0-9.eE+-]+)", r.stdout).group(1))
+    assert err < 1e-3  # np=4 accuracy class (the reference reports ~1.5e-5 on this option set)
 
 
 def test_linearity(gpu):
