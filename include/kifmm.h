@@ -35,7 +35,8 @@ typedef enum {
   KIFMM_ERR_CUDA = 6,        /* a CUDA runtime error (message in kifmm_last_error) */
   KIFMM_ERR_ALLOC = 7,       /* device or host allocation failed */
   KIFMM_ERR_NUMERIC = 8,     /* operator precompute failed (e.g. SVD did not converge) */
-  KIFMM_ERR_NO_DEVICE = 9    /* no CUDA device: there is no CPU fallback */
+  KIFMM_ERR_NO_DEVICE = 9,   /* no CUDA device: there is no CPU fallback */
+  KIFMM_ERR_CAPACITY = 10    /* request larger than kifmm_direct_noalloc's fixed scratch */
 } kifmm_status;
 
 typedef enum {
@@ -99,6 +100,25 @@ kifmm_status kifmm_check(kifmm_handle h, const double* srcden, const double* trg
 /* Replaces Dense3d::eval (fmm3d/dense3d.cpp:38-57) on the device: FP64
  * direct sum from the handle's sources to arbitrary targets (host arrays). */
 kifmm_status kifmm_direct(kifmm_handle h, const double* srcden, int nt, const double* trgpos, double* trgval);
+
+/* No counterpart in the reference.  FP64 direct sum (the kernels of
+ * kifmm_direct) for callers that cannot allocate device memory: a process
+ * whose GPU memory is owned by a framework's caching allocator or a fixed
+ * budget reserved at start-up cannot call cudaMalloc between its steps.
+ * All pointers are device pointers the caller allocated (layouts as in
+ * kifmm_direct); the work is enqueued on `stream` (NULL = legacy default
+ * stream) and the call does not synchronise.  The call allocates nothing:
+ * its partial sums live in one fixed device array of
+ * KIFMM_NOALLOC_SCRATCH_DOUBLES doubles (8 MiB, held on every GPU that loads
+ * the library until exit), so nt * tdof above that limit returns
+ * KIFMM_ERR_CAPACITY.  The first call on a device looks the array up
+ * (cudaGetSymbolAddress) and should come before any stream capture.  All
+ * calls share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller. */
+#define KIFMM_NOALLOC_SCRATCH_DOUBLES (1 << 20)
+kifmm_status kifmm_direct_noalloc(int kt, int ncoef, const double* coefs, int ns, const double* d_srcpos,
+                                  const double* d_srcnor, const double* d_srcden, int nt, const double* d_trgpos,
+                                  double* d_trgval, void* stream);
 
 /* Tree introspection (Let3d, fmm3d/let3d.hpp:38-74), for list parity tests.
  * Nodes are numbered exactly as the reference's breadth-first ndevec. */

@@ -223,6 +223,7 @@ const char* kifmm_status_string(kifmm_status s) {
     case KIFMM_ERR_ALLOC: return "allocation failed";
     case KIFMM_ERR_NUMERIC: return "operator precompute failed";
     case KIFMM_ERR_NO_DEVICE: return "no CUDA device";
+    case KIFMM_ERR_CAPACITY: return "request exceeds the fixed scratch capacity";
   }
   return "unknown status";
 }

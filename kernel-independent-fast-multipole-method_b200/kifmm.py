@@ -28,7 +28,7 @@ LIB_PATH = os.path.join(HERE, "lib", "libkifmm_b200.so")
 
 STATUS = {0: "KIFMM_OK", 1: "KIFMM_ERR_ARG", 2: "KIFMM_ERR_KERNEL", 3: "KIFMM_ERR_OUT_OF_BOX",
           4: "KIFMM_ERR_STATE", 5: "KIFMM_ERR_OPTION", 6: "KIFMM_ERR_CUDA", 7: "KIFMM_ERR_ALLOC",
-          8: "KIFMM_ERR_NUMERIC", 9: "KIFMM_ERR_NO_DEVICE"}
+          8: "KIFMM_ERR_NUMERIC", 9: "KIFMM_ERR_NO_DEVICE", 10: "KIFMM_ERR_CAPACITY"}
 for _c, _n in STATUS.items():
     globals()[_n] = _c
 
@@ -51,6 +51,8 @@ SIGNATURES = {
     "kifmm_eval_device": [_H, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int],
     "kifmm_check": [_H, _DP, _DP, ctypes.c_int, ctypes.c_uint64, _DP],
     "kifmm_direct": [_H, _DP, ctypes.c_int, _DP, _DP],
+    "kifmm_direct_noalloc": [ctypes.c_int, ctypes.c_int, _DP, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                             ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
     "kifmm_tree_size": [_H, _IP, _IP],
     "kifmm_tree_nodes": [_H, _IP, _IP, _IP, _IP, _IP, _IP, _IP],
     "kifmm_tree_lists": [_H, ctypes.c_int, _LP, _LP, _IP],
