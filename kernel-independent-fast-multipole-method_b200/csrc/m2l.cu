@@ -42,16 +42,20 @@ __device__ __forceinline__ void twiddles(Cpx<T>* w, int n) {
 // spectra[node][s][f], f = (kz*n + ky)*nh + kx
 template <typename T>
 __global__ void __launch_bounds__(FFT_THREADS) k_m2l_fwd(M2LGeom g, const T* __restrict__ supeden,
-                                                          const int* __restrict__ nodes, const int* __restrict__ depth,
-                                                          T* __restrict__ spectra) {
+                                                          const int* __restrict__ nodes, int nwork,
+                                                          const int* __restrict__ depth, T* __restrict__ spectra) {
   __shared__ T xg[NPMAX * NPMAX * NPMAX];
   __shared__ Cpx<T> A[NPMAX * NPMAX * NHMAX];  // A[k][j][kx]
   __shared__ Cpx<T> Bm[NPMAX * NMAX * NHMAX];  // B[k][ky][kx]
   __shared__ Cpx<T> w[NMAX];
+  __shared__ Cpx<T> W2[NMAX * NMAX];  // W2[a*n + b] = w^(a*b mod n)
   const int np = g.np, n = g.n, nh = g.nh, nf = g.nfreq;
-  const int node = nodes[blockIdx.x];
-  const int lvl = depth[node] + g.rootlvl;
   twiddles(w, n);
+  __syncthreads();
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) W2[e] = w[((e / n) * (e % n)) % n];
+  for (int wi = blockIdx.x; wi < nwork; wi += gridDim.x) {
+  const int node = nodes[wi];
+  const int lvl = depth[node] + g.rootlvl;
   const T* den = supeden + (size_t)node * g.nsurf * g.sd;
   for (int s = 0; s < g.sd; s++) {
     T scale = (T)ldexp(1.0, lvl * g.deg[s]);  // plnden2effden scaling, matmgnt3d.cpp:228-235
@@ -68,7 +72,7 @@ __global__ void __launch_bounds__(FFT_THREADS) k_m2l_fwd(M2LGeom g, const T* __r
       T re = 0, im = 0;
       for (int i = 0; i < np; i++) {
         T v = xg[(i * np + j) * np + k];
-        Cpx<T> t = w[(i * kx) % n];
+        Cpx<T> t = W2[i * n + kx];
         re += v * t.re;
         im += v * t.im;
       }
@@ -82,7 +86,7 @@ __global__ void __launch_bounds__(FFT_THREADS) k_m2l_fwd(M2LGeom g, const T* __r
       T re = 0, im = 0;
       for (int j = 0; j < np; j++) {
         Cpx<T> a = A[(k * np + j) * nh + kx];
-        Cpx<T> t = w[(j * ky) % n];
+        Cpx<T> t = W2[j * n + ky];
         re += a.re * t.re - a.im * t.im;
         im += a.re * t.im + a.im * t.re;
       }
@@ -97,7 +101,7 @@ __global__ void __launch_bounds__(FFT_THREADS) k_m2l_fwd(M2LGeom g, const T* __r
       T re = 0, im = 0;
       for (int k = 0; k < np; k++) {
         Cpx<T> b = Bm[k * n * nh + kxy];
-        Cpx<T> t = w[(k * kz) % n];
+        Cpx<T> t = W2[k * n + kz];
         re += b.re * t.re - b.im * t.im;
         im += b.re * t.im + b.im * t.re;
       }
@@ -105,6 +109,7 @@ __global__ void __launch_bounds__(FFT_THREADS) k_m2l_fwd(M2LGeom g, const T* __r
       out[2 * e + 1] = im;
     }
     __syncthreads();
+  }
   }
 }
 
@@ -270,7 +275,8 @@ __global__ void __launch_bounds__(256) k_m2l_had_pairs(int nf, const T* __restri
 // tdncval[node][m][t] += real inverse transform of effval at the surface points
 template <typename T>
 __global__ void __launch_bounds__(FFT_THREADS) k_m2l_inv(M2LGeom g, const T* __restrict__ effval,
-                                                          const int* __restrict__ work, T* __restrict__ tdncval) {
+                                                          const int* __restrict__ work, int nwork,
+                                                          T* __restrict__ tdncval) {
   // dynamic shared memory: Y[n*n*nh] | B[np*n*nh] | A[np*np*nh] | w[n]
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int np = g.np, n = g.n, nh = g.nh, nf = g.nfreq;
@@ -278,9 +284,12 @@ __global__ void __launch_bounds__(FFT_THREADS) k_m2l_inv(M2LGeom g, const T* __r
   Cpx<T>* Bm = Y + n * n * nh;
   Cpx<T>* A = Bm + np * n * nh;
   Cpx<T>* w = A + np * np * nh;
-  const int wi = blockIdx.x;
-  const int node = work[wi];
+  Cpx<T>* W2 = w + n;  // W2[a*n + b] = w^(a*b mod n)
   twiddles(w, n);
+  __syncthreads();
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) W2[e] = w[((e / n) * (e % n)) % n];
+  for (int wi = blockIdx.x; wi < nwork; wi += gridDim.x) {
+  const int node = work[wi];
   for (int t = 0; t < g.td; t++) {
     const T* src = effval + ((size_t)node * g.td + t) * nf * 2;
     for (int e = threadIdx.x; e < nf; e += blockDim.x) {
@@ -294,7 +303,7 @@ __global__ void __launch_bounds__(FFT_THREADS) k_m2l_inv(M2LGeom g, const T* __r
       T re = 0, im = 0;
       for (int kz = 0; kz < n; kz++) {
         Cpx<T> y = Y[kz * n * nh + kxy];
-        Cpx<T> c = w[(k * kz) % n];
+        Cpx<T> c = W2[k * n + kz];
         re += y.re * c.re + y.im * c.im;
         im += y.im * c.re - y.re * c.im;
       }
@@ -308,7 +317,7 @@ __global__ void __launch_bounds__(FFT_THREADS) k_m2l_inv(M2LGeom g, const T* __r
       T re = 0, im = 0;
       for (int ky = 0; ky < n; ky++) {
         Cpx<T> b = Bm[(k * n + ky) * nh + kx];
-        Cpx<T> c = w[(j * ky) % n];
+        Cpx<T> c = W2[j * n + ky];
         re += b.re * c.re + b.im * c.im;
         im += b.im * c.re - b.re * c.im;
       }
@@ -324,12 +333,13 @@ __global__ void __launch_bounds__(FFT_THREADS) k_m2l_inv(M2LGeom g, const T* __r
       T v = a[0].re + ((i & 1) ? -a[nh - 1].re : a[nh - 1].re);
       T acc = 0;
       for (int kx = 1; kx < nh - 1; kx++) {
-        Cpx<T> c = w[(i * kx) % n];
+        Cpx<T> c = W2[i * n + kx];
         acc += a[kx].re * c.re + a[kx].im * c.im;  // Re(a * conj(w)^(i kx))
       }
       dst[(size_t)m * g.td + t] += v + T(2) * acc;
     }
     __syncthreads();
+  }
   }
 }
 
@@ -339,7 +349,7 @@ template <typename T>
 void launch_m2l_forward(const M2LGeom& g, const T* supeden, const int* nodes, int nn, const int* depth, T* spectra,
                         cudaStream_t st) {
   if (nn <= 0) return;
-  k_m2l_fwd<T><<<nn, FFT_THREADS, 0, st>>>(g, supeden, nodes, depth, spectra);
+  k_m2l_fwd<T><<<std::min(nn, 148 * 16), FFT_THREADS, 0, st>>>(g, supeden, nodes, nn, depth, spectra);
 }
 
 template <typename T>
@@ -357,25 +367,142 @@ void launch_m2l_hadamard(const M2LGeom& g, const T* khat, const T* spectra, cons
 template <typename T>
 void launch_m2l_inverse(const M2LGeom& g, const T* effval, const int* work, int nwork, T* tdncval, cudaStream_t st) {
   if (nwork <= 0) return;
-  size_t smem = sizeof(Cpx<T>) * ((size_t)g.n * g.n * g.nh + (size_t)g.np * g.n * g.nh + (size_t)g.np * g.np * g.nh + g.n);
+  size_t smem = sizeof(Cpx<T>) * ((size_t)g.n * g.n * g.nh + (size_t)g.np * g.n * g.nh + (size_t)g.np * g.np * g.nh +
+                                  g.n + (size_t)g.n * g.n);
   if (smem > 48 * 1024) cudaFuncSetAttribute(k_m2l_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_m2l_inv<T><<<nwork, FFT_THREADS, smem, st>>>(g, effval, work, tdncval);
+  k_m2l_inv<T><<<std::min(nwork, 148 * 8), FFT_THREADS, smem, st>>>(g, effval, work, nwork, tdncval);
+}
+
+// Persistent form: each CTA owns a contiguous slice of target parents (Morton
+// order, so neighbouring parents share colleagues) and sweeps the frequency
+// tiles in order.  All CTAs therefore work on about the same tile at the same
+// time and its source spectra (nodes x 32 freq x 8 B, ~93 MB at 4M points)
+// stay in L2 for their 26-fold reuse.  The next colleague's 8 child spectra
+// are loaded into registers while the current colleague is multiplied.
+template <typename T, int QPT>
+__global__ void __launch_bounds__(256) k_m2l_had_sweep(int nf, const T* __restrict__ khat_c,
+                                                       const T* __restrict__ spectra, int nq,
+                                                       const int* __restrict__ qchd, const int* __restrict__ coll,
+                                                       const unsigned char* __restrict__ mask,
+                                                       T* __restrict__ effval) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Cpx<T>* Ks = reinterpret_cast<Cpx<T>*>(smem_raw);  // [316][32]
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int per_cta = (nq + gridDim.x - 1) / gridDim.x;
+  const int qbeg = blockIdx.x * per_cta;
+  const int qend = min(nq, qbeg + per_cta);
+  const int ftiles = (nf + 31) / 32;
+  for (int ft = 0; ft < ftiles; ft++) {
+    const int f0 = ft * 32;
+    const int f = f0 + lane;
+    const bool fv = f < nf;
+    __syncthreads();
+    for (int e = threadIdx.x; e < 316 * 32; e += blockDim.x) {
+      int o = e >> 5, l = e & 31;
+      Cpx<T> v;
+      v.re = v.im = T(0);
+      if (f0 + l < nf) {
+        v.re = khat_c[((size_t)o * nf + f0 + l) * 2];
+        v.im = khat_c[((size_t)o * nf + f0 + l) * 2 + 1];
+      }
+      Ks[e] = v;
+    }
+    __syncthreads();
+    for (int q0 = qbeg + warp * QPT; q0 < qend; q0 += 8 * QPT) {
+      T ar[QPT][8], ai[QPT][8];
+#pragma unroll
+      for (int q = 0; q < QPT; q++)
+#pragma unroll
+        for (int i = 0; i < 8; i++) ar[q][i] = ai[q][i] = T(0);
+      // prefetch colleague 0
+      int nb[QPT];
+      T nxr[QPT][8], nxi[QPT][8];
+#pragma unroll
+      for (int q = 0; q < QPT; q++) nb[q] = (q0 + q < qend) ? coll[(size_t)(q0 + q) * 26] : -1;
+#pragma unroll
+      for (int q = 0; q < QPT; q++)
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+          nxr[q][j] = nxi[q][j] = T(0);
+          if (nb[q] >= 0 && fv) {
+            const T* X = spectra + ((size_t)(nb[q] + j) * nf + f) * 2;
+            nxr[q][j] = X[0];
+            nxi[q][j] = X[1];
+          }
+        }
+      for (int dir = 0; dir < 26; dir++) {
+        T xr[QPT][8], xi[QPT][8];
+        bool any = false;
+#pragma unroll
+        for (int q = 0; q < QPT; q++) {
+          any |= nb[q] >= 0;
+#pragma unroll
+          for (int j = 0; j < 8; j++) {
+            xr[q][j] = nxr[q][j];
+            xi[q][j] = nxi[q][j];
+          }
+        }
+        if (dir + 1 < 26) {
+#pragma unroll
+          for (int q = 0; q < QPT; q++) nb[q] = (q0 + q < qend) ? coll[(size_t)(q0 + q) * 26 + dir + 1] : -1;
+#pragma unroll
+          for (int q = 0; q < QPT; q++)
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+              nxr[q][j] = nxi[q][j] = T(0);
+              if (nb[q] >= 0 && fv) {
+                const T* X = spectra + ((size_t)(nb[q] + j) * nf + f) * 2;
+                nxr[q][j] = X[0];
+                nxi[q][j] = X[1];
+              }
+            }
+        }
+        if (!any) continue;
+        const short* offs = &c_pair_off[dir * 64];
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+#pragma unroll
+          for (int i = 0; i < 8; i++) {
+            int o = offs[i * 8 + j];
+            if (o < 0) continue;
+            Cpx<T> k = Ks[o * 32 + lane];
+#pragma unroll
+            for (int q = 0; q < QPT; q++) {
+              ar[q][i] += k.re * xr[q][j] - k.im * xi[q][j];
+              ai[q][i] += k.re * xi[q][j] + k.im * xr[q][j];
+            }
+          }
+        }
+      }
+      if (fv) {
+#pragma unroll
+        for (int q = 0; q < QPT; q++) {
+          if (q0 + q >= qend) continue;
+          int c0 = qchd[q0 + q];
+          unsigned m = mask[q0 + q];
+#pragma unroll
+          for (int i = 0; i < 8; i++) {
+            if (!((m >> i) & 1)) continue;
+            T* Y = effval + ((size_t)(c0 + i) * nf + f) * 2;
+            Y[0] = ar[q][i];
+            Y[1] = ai[q][i];
+          }
+        }
+      }
+    }
+  }
 }
 
 template <typename T>
 void launch_m2l_hadamard_pairs(int nf, const T* khat_c, const T* spectra, int nq, const int* qchd, const int* coll,
                                const unsigned char* mask, T* effval, int num_sms, cudaStream_t st) {
   if (nq <= 0) return;
-  constexpr int QPT = sizeof(T) == 4 ? 4 : 2;
+  constexpr int QPT = 2;
   size_t smem = sizeof(Cpx<T>) * 316 * 32;
-  cudaFuncSetAttribute(k_m2l_had_pairs<T, QPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  int ftiles = (nf + 31) / 32;
+  cudaFuncSetAttribute(k_m2l_had_sweep<T, QPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int per_sm = sizeof(T) == 4 ? 2 : 1;
-  int qchunks = std::max(1, (num_sms * per_sm + ftiles - 1) / ftiles);
-  int warps_needed = (nq + QPT - 1) / QPT;
-  qchunks = std::min(qchunks, std::max(1, (warps_needed + 7) / 8));
-  dim3 grid(ftiles, qchunks);
-  k_m2l_had_pairs<T, QPT><<<grid, 256, smem, st>>>(nf, khat_c, spectra, nq, qchd, coll, mask, effval);
+  int grid = std::max(1, std::min(num_sms * per_sm, (nq + 8 * QPT - 1) / (8 * QPT)));
+  k_m2l_had_sweep<T, QPT><<<grid, 256, smem, st>>>(nf, khat_c, spectra, nq, qchd, coll, mask, effval);
 }
 
 void m2l_set_pair_table(const short* tab, cudaStream_t st) {
