@@ -338,7 +338,6 @@ struct Impl : ImplBase {
   int pairs_n = 0, num_sms = 148;
   int *pairs_chd = nullptr, *pairs_coll = nullptr;
   unsigned char* pairs_mask = nullptr;
-  T* khat_c = nullptr;
 
   void build_pairs(const std::vector<int>& vtargets) {
     const Csr& V = tr.lists[1];
@@ -400,15 +399,6 @@ struct Impl : ImplBase {
         }
       }
     }
-    std::vector<T> kc((size_t)316 * op.nfreq * 2);
-    for (int oi = 0; oi < 343; oi++) {
-      if (compact[oi] < 0) continue;
-      for (int f = 0; f < op.nfreq; f++) {
-        kc[((size_t)compact[oi] * op.nfreq + f) * 2] = (T)op.m2l[(size_t)oi * op.nfreq + f].real();
-        kc[((size_t)compact[oi] * op.nfreq + f) * 2 + 1] = (T)op.m2l[(size_t)oi * op.nfreq + f].imag();
-      }
-    }
-    khat_c = upload(kc);
     pairs_chd = upload(qchd);
     pairs_coll = upload(coll);
     pairs_mask = upload(mask);
@@ -496,7 +486,7 @@ struct Impl : ImplBase {
         launch_m2l_forward<T>(geom, supeden, fwd.work, fwd.n, d_depth, spectra, st);
         if (prof && r == 0) KCHECK(cudaEventRecord(ev[7], st));
         if (pairs_n > 0)
-          launch_m2l_hadamard_pairs<T>(op.nfreq, khat_c, spectra, pairs_n, pairs_chd, pairs_coll, pairs_mask, effval,
+          launch_m2l_hadamard_pairs<T>(op.nfreq, khat, spectra, pairs_n, pairs_chd, pairs_coll, pairs_mask, effval,
                                        num_sms, st);
         else
           launch_m2l_hadamard<T>(geom, khat, spectra, m2l.work, m2l.n, m2l.ptr, m2l.idx, d_path, effval, st);

@@ -379,15 +379,16 @@ void launch_m2l_inverse(const M2LGeom& g, const T* effval, const int* work, int 
 // time and its source spectra (nodes x 32 freq x 8 B, ~93 MB at 4M points)
 // stay in L2 for their 26-fold reuse.  The next colleague's 8 child spectra
 // are loaded into registers while the current colleague is multiplied.
-template <typename T, int QPT>
-__global__ void __launch_bounds__(256) k_m2l_had_sweep(int nf, const T* __restrict__ khat_c,
+template <typename T, int QPT, int NTHR>
+__global__ void __launch_bounds__(NTHR) k_m2l_had_sweep(int nf, const T* __restrict__ khat,
                                                        const T* __restrict__ spectra, int nq,
                                                        const int* __restrict__ qchd, const int* __restrict__ coll,
                                                        const unsigned char* __restrict__ mask,
                                                        T* __restrict__ effval) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  Cpx<T>* Ks = reinterpret_cast<Cpx<T>*>(smem_raw);  // [316][32]
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  Cpx<T>* Ks = reinterpret_cast<Cpx<T>*>(smem_raw);  // [343][32]: every offset in [-3,3]^3, zero when |o| <= 1
+  __shared__ int next_q;  // next unclaimed group of the CTA's slice, per frequency tile
+  const int lane = threadIdx.x & 31;
   const int per_cta = (nq + gridDim.x - 1) / gridDim.x;
   const int qbeg = blockIdx.x * per_cta;
   const int qend = min(nq, qbeg + per_cta);
@@ -397,18 +398,24 @@ __global__ void __launch_bounds__(256) k_m2l_had_sweep(int nf, const T* __restri
     const int f = f0 + lane;
     const bool fv = f < nf;
     __syncthreads();
-    for (int e = threadIdx.x; e < 316 * 32; e += blockDim.x) {
+    if (threadIdx.x == 0) next_q = qbeg;
+    for (int e = threadIdx.x; e < 343 * 32; e += blockDim.x) {
       int o = e >> 5, l = e & 31;
       Cpx<T> v;
       v.re = v.im = T(0);
       if (f0 + l < nf) {
-        v.re = khat_c[((size_t)o * nf + f0 + l) * 2];
-        v.im = khat_c[((size_t)o * nf + f0 + l) * 2 + 1];
+        v.re = khat[((size_t)o * nf + f0 + l) * 2];
+        v.im = khat[((size_t)o * nf + f0 + l) * 2 + 1];
       }
       Ks[e] = v;
     }
     __syncthreads();
-    for (int q0 = qbeg + warp * QPT; q0 < qend; q0 += 8 * QPT) {
+    // warps claim QPT target parents at a time, so they finish the tile together
+    while (true) {
+      int q0 = 0;
+      if (lane == 0) q0 = atomicAdd(&next_q, QPT);
+      q0 = __shfl_sync(0xffffffffu, q0, 0);
+      if (q0 >= qend) break;
       T ar[QPT][8], ai[QPT][8];
 #pragma unroll
       for (int q = 0; q < QPT; q++)
@@ -458,14 +465,18 @@ __global__ void __launch_bounds__(256) k_m2l_had_sweep(int nf, const T* __restri
             }
         }
         if (!any) continue;
-        const short* offs = &c_pair_off[dir * 64];
+        // offset of child j of P from child i of Q: 2*dir + oct(j) - oct(i); the
+        // adjacent pairs (|offset| <= 1) read the zero rows of the tile
+        const int dd = dir < 13 ? dir : dir + 1;
+        const int base = (2 * (dd / 9 - 1) + 3) * 49 + (2 * ((dd / 3) % 3 - 1) + 3) * 7 + (2 * (dd % 3 - 1) + 3);
+        const Cpx<T>* Kd = Ks + base * 32 + lane;
 #pragma unroll
         for (int j = 0; j < 8; j++) {
 #pragma unroll
           for (int i = 0; i < 8; i++) {
-            int o = offs[i * 8 + j];
-            if (o < 0) continue;
-            Cpx<T> k = Ks[o * 32 + lane];
+            const int cij = (((j >> 2) & 1) - ((i >> 2) & 1)) * 49 + (((j >> 1) & 1) - ((i >> 1) & 1)) * 7 +
+                            ((j & 1) - (i & 1));
+            Cpx<T> k = Kd[cij * 32];
 #pragma unroll
             for (int q = 0; q < QPT; q++) {
               ar[q][i] += k.re * xr[q][j] - k.im * xi[q][j];
@@ -494,15 +505,16 @@ __global__ void __launch_bounds__(256) k_m2l_had_sweep(int nf, const T* __restri
 }
 
 template <typename T>
-void launch_m2l_hadamard_pairs(int nf, const T* khat_c, const T* spectra, int nq, const int* qchd, const int* coll,
+void launch_m2l_hadamard_pairs(int nf, const T* khat, const T* spectra, int nq, const int* qchd, const int* coll,
                                const unsigned char* mask, T* effval, int num_sms, cudaStream_t st) {
   if (nq <= 0) return;
   constexpr int QPT = 2;
-  size_t smem = sizeof(Cpx<T>) * 316 * 32;
-  cudaFuncSetAttribute(k_m2l_had_sweep<T, QPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  int per_sm = sizeof(T) == 4 ? 2 : 1;
-  int grid = std::max(1, std::min(num_sms * per_sm, (nq + 8 * QPT - 1) / (8 * QPT)));
-  k_m2l_had_sweep<T, QPT><<<grid, 256, smem, st>>>(nf, khat_c, spectra, nq, qchd, coll, mask, effval);
+  size_t smem = sizeof(Cpx<T>) * 343 * 32;
+  // one CTA per SM: 16 warps (FP32) or 8 warps (FP64, twice the registers) share one operator tile
+  constexpr int NTHR = sizeof(T) == 4 ? 512 : 256;
+  cudaFuncSetAttribute(k_m2l_had_sweep<T, QPT, NTHR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int grid = std::max(1, std::min(num_sms, (nq + QPT - 1) / QPT));
+  k_m2l_had_sweep<T, QPT, NTHR><<<grid, NTHR, smem, st>>>(nf, khat, spectra, nq, qchd, coll, mask, effval);
 }
 
 void m2l_set_pair_table(const short* tab, cudaStream_t st) {
