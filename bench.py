@@ -10,7 +10,12 @@ point cloud; setup (tree, lists, operators) is done once, outside timing.
   value      Mpoints/s of the mixed-precision engine (FP32 bulk, FP64
              pseudo-inverse products), all ranks together
   fp64       the plain FP64 GPU engine on the same workload
-  e2e        Mpoints/s through the host-pointer C API (kifmm_eval): H2D of the
+  batched    64 independent instances (48 Laplace + 16 Stokes single-layer,
+             np=6, log-uniform sizes in [1e4, 5e5], sphere / cube / Plummer
+             ball), 8 density vectors each, as one captured CUDA graph:
+             aggregate point-evaluations/s, mixed and FP64, with per-instance
+             errors against the direct sum
+  e2e       Mpoints/s through the host-pointer C API (kifmm_eval): H2D of the
              densities and D2H of the potentials inside the timed region
   relerr     ||fmm - direct|| / ||fmm|| at 4096 check targets against the
              FP64 direct sum (the reference's FMM3d::check metric)
@@ -61,6 +66,7 @@ def parse():
     ap.add_argument("--n", type=int, default=N_POINTS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
     return ap.parse_args()
 
 
@@ -198,6 +204,76 @@ def peaks():
         return 6650.0, "fallback"
 
 
+BATCH_RHS = 8
+BATCH_NCHK = 256
+
+
+def batched_section(torch, kifmm, stream, flush, steps, warmup, precision, pg=None):
+    """64 independent instances (48 Laplace + 16 Stokes single-layer, np=6,
+    log-uniform sizes in [1e4, 5e5], sphere / cube / Plummer ball), 8 density
+    vectors each, evaluated as one captured CUDA graph (kifmm_batch_eval_device).
+    Returns the aggregate point-evaluations per second and per-instance errors
+    against the FP64 direct sum (first and last density vector, 256 targets)."""
+    insts = W.batched_instances()
+    fmms, srcs, outs, dens, pts = [], [], [], [], []
+    t0 = time.perf_counter()
+    for inst in insts:
+        p, _ = W.GEOMETRIES[inst["geometry"]](inst["n"], inst["seed"])
+        f = kifmm.FMM3d("fmm3d_")
+        f.srcpos = f.srcnor = f.trgpos = p
+        f.knl = kifmm.Kernel3d(inst["kt"], list(inst["coefs"]))
+        o = dict(OPTS)
+        o["-fmm3d_precision"] = precision
+        f.setup(o)
+        sd, td = W.KERNEL_DOFS[inst["kt"]]
+        den = W.densities(inst["n"] * BATCH_RHS, sd, "uniform", inst["seed"] + 1)
+        fmms.append(f)
+        dens.append(den)
+        pts.append(p)
+        srcs.append(torch.tensor(den, device="cuda", dtype=torch.float64))
+        outs.append(torch.zeros(inst["n"] * td * BATCH_RHS, device="cuda", dtype=torch.float64))
+    setup_s = time.perf_counter() - t0
+    b = kifmm.Batch(fmms)
+    sp, op = [s.data_ptr() for s in srcs], [o.data_ptr() for o in outs]
+    for _ in range(warmup):
+        b.eval(sp, op, BATCH_RHS, stream.cuda_stream, sync=True)
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        b.eval(sp, op, BATCH_RHS, stream.cuda_stream, sync=False)
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    ms = statistics.mean(times)
+    if pg is not None:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+    launches = int(sum(f.last_launch_count() for f in fmms))
+    world = pg.get_world_size() if pg is not None else 1
+    errs = []
+    for inst, f, den, p, out in zip(insts, fmms, dens, pts, outs):
+        n = inst["n"]
+        sd, td = W.KERNEL_DOFS[inst["kt"]]
+        chk = W.check_indices(n, BATCH_NCHK, inst["seed"] + 2)
+        val = out.cpu().numpy().reshape(BATCH_RHS, n, td)
+        for r in (0, BATCH_RHS - 1):
+            direct = f.direct(den[r * n * sd:(r + 1) * n * sd], p[chk]).reshape(-1, td)
+            got = val[r][chk]
+            errs.append(float(np.linalg.norm(direct - got) / np.linalg.norm(got)))
+    npts = sum(i["n"] for i in insts)
+    del b
+    return {"value": world * npts * BATCH_RHS / (ms / 1e3) / 1e6, "unit": "Mpoints/s", "ms_per_step": ms,
+            "relerr_max": max(errs), "relerr_median": statistics.median(errs), "setup_s": setup_s,
+            "launches_per_step": launches, "points_per_instance_total": npts}
+
+
 def engine_arm(args):
     import torch
     import kifmm
@@ -305,6 +381,17 @@ def engine_arm(args):
         fp64 = {"value": world * n / (ms64 / 1e3) / 1e6, "unit": "Mpoints/s", "ms_per_step": ms64,
                 "relerr": err64, "setup_s": setup_fp64, "dtype": "f64"}
         del f64
+    # ---- batched form: 64 instances x 8 density vectors in one graph
+    batched = None
+    if not args.no_batched:
+        bsteps, bwarm = max(1, min(args.steps, 5)), max(1, min(args.warmup, 3))
+        batched = {"workload": "batched_64x8rhs_np6", "instances": 64, "rhs": BATCH_RHS,
+                   "kernels": "48 x Laplace SL (111), 16 x Stokes SL (311)",
+                   "sizes": "log-uniform in [1e4, 5e5] points", "geometries": "sphere / cube / Plummer ball",
+                   "check": f"{BATCH_NCHK} targets per instance, density vectors 0 and {BATCH_RHS - 1}",
+                   "mixed": batched_section(torch, kifmm, stream, flush, bsteps, bwarm, "mixed", pg)}
+        if not args.no_fp64:
+            batched["fp64"] = batched_section(torch, kifmm, stream, flush, bsteps, bwarm, "fp64", pg)
     # ---- CPU baseline: the reference on a bounded sample, rank 0, N=1
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -339,6 +426,7 @@ def engine_arm(args):
                    "l2": "flushed (256 MB write) before every timed step", "parallelism": f"replicas x{world}"},
         "relerr": relerr, "check_targets": NCHK,
         "fp64": fp64,
+        "batched": batched,
         "e2e": {"value": world * n / (e2e_ms / 1e3) / 1e6, "unit": "Mpoints/s",
                 "h2d_bytes_per_step": int(n * 8), "d2h_bytes_per_step": int(n * 8), "ms_per_step": e2e_ms},
         "gpu_launches": int(launches * args.steps),

@@ -91,6 +91,21 @@ kifmm_status kifmm_eval_multi(kifmm_handle h, int nrhs, const double* srcden, do
 kifmm_status kifmm_eval_device(kifmm_handle h, int nrhs, const double* d_srcden, double* d_trgval, void* stream,
                                int sync);
 
+/* Batched evaluation of independent instances (no counterpart in the
+ * reference, which runs one FMM3d::eval at a time, fmm3d/tt.cpp:97-101).
+ * A batch groups already set-up handles (any kernels and sizes); each
+ * kifmm_batch_eval_device call evaluates nrhs density vectors for every
+ * instance (device pointers d_srcden[i] / d_trgval[i], layouts as in
+ * kifmm_eval_device).  The instances run concurrently, and the whole batch is
+ * captured into one CUDA graph on the first call and replayed while nrhs and
+ * the pointers stay the same. */
+typedef struct kifmm_batch_s* kifmm_batch;
+kifmm_status kifmm_batch_create(int n, const kifmm_handle* handles, kifmm_batch* out);
+kifmm_status kifmm_batch_destroy(kifmm_batch b);
+kifmm_status kifmm_batch_eval_device(kifmm_batch b, int nrhs, const double* const* d_srcden,
+                                     double* const* d_trgval, void* stream, int sync);
+const char* kifmm_batch_last_error(kifmm_batch b);
+
 /* Replaces FMM3d::check(srcden, trgval, numchk) (fmm3d/fmm3d_check.cpp:25-73):
  * FP64 direct sum at numchk targets picked with `seed`; returns
  * ||fmm - direct|| / ||fmm|| in *relerr (the reference's metric, :61-71). */

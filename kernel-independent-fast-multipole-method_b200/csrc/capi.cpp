@@ -6,10 +6,6 @@
 #include "../../include/kifmm.h"
 #include "engine.hpp"
 
-struct kifmm_engine {
-  kifmm::Engine e;
-};
-
 using kifmm::Engine;
 
 namespace {

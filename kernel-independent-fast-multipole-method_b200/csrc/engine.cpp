@@ -91,10 +91,15 @@ struct Impl : ImplBase {
   T *sden = nullptr, *tval = nullptr;
   int cap_rhs = 0;
   T *supeden, *supcval, *tdncval, *tdneden, *spectra, *effval;
-  double *A_uc2ue, *A_m2m, *A_dc2de, *A_l2l;  // FP64 in both precisions (see gemm.cu)
+  T *A_upW, *A_upV, *A_m2my, *A_dnW, *A_dnV, *A_l2lz;  // factored surface operators
+  T *ybuf, *zbuf;  // per-node rank-space coordinates of the upward / downward densities
+  int ru = 0, rd = 0;
   T* khat;
   List s2m, s2l, leaf, m2l, fwd;
-  std::vector<List> up_leaf, up_non, dn, dn_par;
+  std::vector<List> up_non, dn_par;
+  List up_all, dn_all;
+  double* gemm_ws = nullptr;
+  size_t gemm_ws_len = 0;
   cudaEvent_t ev[9];  // phase boundaries + the two interior V-list kernel boundaries
   bool have_events = false;
   int nlaunch = 0;
@@ -168,10 +173,14 @@ struct Impl : ImplBase {
     args.uc_unit = upload_as_T(op.uc);
     args.de_unit = upload_as_T(op.de);
     args.dc_unit = upload_as_T(op.dc);
-    A_uc2ue = upload(op.uc2ue);
-    A_m2m = upload(op.m2m);
-    A_dc2de = upload(op.dc2de);
-    A_l2l = upload(op.l2l);
+    ru = op.rank_up;
+    rd = op.rank_dn;
+    A_upW = upload_as_T(op.up_W);
+    A_upV = upload_as_T(op.up_V);
+    A_m2my = upload_as_T(op.m2m_y);
+    A_dnW = upload_as_T(op.dn_W);
+    A_dnV = upload_as_T(op.dn_V);
+    A_l2lz = upload_as_T(op.l2l_z);
     {
       std::vector<T> kh(op.m2l.size() * 2);
       for (size_t i = 0; i < op.m2l.size(); i++) {
@@ -192,6 +201,12 @@ struct Impl : ImplBase {
     tdncval = dalloc<T>((size_t)nn * nsurf * td_m);
     tdneden = dalloc<T>((size_t)nn * nsurf * sd_m);
     KCHECK(cudaMemset(tdneden, 0, sizeof(T) * (size_t)nn * nsurf * sd_m));
+    // y of a source-free child stays zero; z of a target-free child is written
+    // by the L2L chain but never read
+    ybuf = dalloc<T>((size_t)nn * ru);
+    KCHECK(cudaMemset(ybuf, 0, sizeof(T) * (size_t)nn * ru));
+    zbuf = dalloc<T>((size_t)nn * rd);
+    KCHECK(cudaMemset(zbuf, 0, sizeof(T) * (size_t)nn * rd));
     args.supeden = supeden;
     args.supcval = supcval;
     args.tdncval = tdncval;
@@ -199,24 +214,19 @@ struct Impl : ImplBase {
 
     // ---- work lists
     const int md = tr.maxdepth;
-    up_leaf.resize(md + 1);
     up_non.resize(md + 1);
-    dn.resize(md + 1);
     dn_par.resize(md + 1);
     std::vector<int> v_s2m;
     for (int d = 2; d <= md; d++) {
-      std::vector<int> ul, un, unc, dd, dp, dpc;
+      std::vector<int> un, unc, dp, dpc;
       for (int g = tr.level_beg[d]; g < tr.level_beg[d + 1]; g++) {
-        if (tr.tag[g] & TAG_SRC) {
-          if (tr.terminal(g)) {
-            ul.push_back(g);
-            v_s2m.push_back(g);
-          } else {
-            un.push_back(g);
-            unc.push_back(tr.chd[g]);
-          }
+        if (!(tr.tag[g] & TAG_SRC)) continue;
+        if (tr.terminal(g)) {
+          v_s2m.push_back(g);
+        } else {
+          un.push_back(g);
+          unc.push_back(tr.chd[g]);
         }
-        if (tr.tag[g] & TAG_TRG) dd.push_back(g);
       }
       if (d >= 3)
         for (int g = tr.level_beg[d - 1]; g < tr.level_beg[d]; g++)
@@ -224,12 +234,33 @@ struct Impl : ImplBase {
             dp.push_back(g);
             dpc.push_back(tr.chd[g]);
           }
-      up_leaf[d] = make_list(ul, {});
       up_non[d] = make_list(un, unc);
-      dn[d] = make_list(dd, {});
       dn_par[d] = make_list(dp, dpc);
     }
-    s2m = make_list(v_s2m, {});
+    {
+      // all-level lists (aux = node depth): source leaves, every upward node,
+      // every downward node
+      std::vector<int> s2m_lvl, all_up, all_up_lvl, all_dn, all_dn_lvl;
+      for (int g : v_s2m) s2m_lvl.push_back(tr.depth[g]);
+      for (int d = 2; d <= md; d++)
+        for (int g = tr.level_beg[d]; g < tr.level_beg[d + 1]; g++)
+          if (tr.tag[g] & TAG_SRC) {
+            all_up.push_back(g);
+            all_up_lvl.push_back(d);
+          }
+      for (int d = 2; d <= md; d++)
+        for (int g = tr.level_beg[d]; g < tr.level_beg[d + 1]; g++)
+          if (tr.tag[g] & TAG_TRG) {
+            all_dn.push_back(g);
+            all_dn_lvl.push_back(d);
+          }
+      s2m = make_list(v_s2m, s2m_lvl);
+      up_all = make_list(all_up, all_up_lvl);
+      dn_all = make_list(all_dn, all_dn_lvl);
+      KCHECK(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, E.device));
+      gemm_ws_len = (size_t)4 << 20;  // split-K slices of the shallow levels (32 MB)
+      gemm_ws = dalloc<double>(gemm_ws_len);
+    }
     // V list (M2L), forward set
     {
       std::vector<int> work, fwdn;
@@ -320,12 +351,11 @@ struct Impl : ImplBase {
     scl.sd = sd_m;
     for (int s = 0; s < sd_m && s < 4; s++) scl.deg[s] = op.deg[s];
     // GEMM flops per eval
-    double gf = 0;
+    double gf = 2.0 * ru * (nuc * td_m) * s2m.n + 2.0 * (nsurf * sd_m) * ru * up_all.n +
+                2.0 * rd * (nsurf * td_m) * dn_all.n + 2.0 * (nsurf * sd_m) * rd * dn_all.n;
     for (int d = 2; d <= md; d++) {
-      gf += 2.0 * (nsurf * sd_m) * (nuc * td_m) * up_leaf[d].n;
-      gf += 2.0 * (nsurf * sd_m) * (8.0 * nsurf * sd_m) * up_non[d].n;
-      gf += 2.0 * (nsurf * sd_m) * (nsurf * td_m) * dn[d].n;
-      gf += 2.0 * (8.0 * nsurf * sd_m) * (nsurf * sd_m) * dn_par[d].n;
+      gf += 2.0 * ru * (8.0 * ru) * up_non[d].n;
+      gf += 2.0 * (8.0 * rd) * rd * dn_par[d].n;
     }
     counters_gemm = gf;
     for (auto& x : ev) KCHECK(cudaEventCreate(&x));
@@ -341,33 +371,6 @@ struct Impl : ImplBase {
 
   void build_pairs(const std::vector<int>& vtargets) {
     const Csr& V = tr.lists[1];
-    // compact offsets (max |o| >= 2) and the [dir][i][j] table
-    std::vector<int> compact(343, -1);
-    int nc = 0;
-    for (int ox = -3; ox <= 3; ox++)
-      for (int oy = -3; oy <= 3; oy++)
-        for (int oz = -3; oz <= 3; oz++)
-          if (std::max(std::abs(ox), std::max(std::abs(oy), std::abs(oz))) > 1) compact[offset_index(ox, oy, oz)] = nc++;
-    std::vector<short> tab(26 * 64, -1);
-    int dirs[26][3], nd = 0;
-    for (int dx = -1; dx <= 1; dx++)
-      for (int dy = -1; dy <= 1; dy++)
-        for (int dz = -1; dz <= 1; dz++)
-          if (dx || dy || dz) {
-            dirs[nd][0] = dx;
-            dirs[nd][1] = dy;
-            dirs[nd][2] = dz;
-            nd++;
-          }
-    for (int d = 0; d < 26; d++)
-      for (int i = 0; i < 8; i++)
-        for (int j = 0; j < 8; j++) {
-          int o[3];
-          for (int a = 0; a < 3; a++) o[a] = 2 * dirs[d][a] + ((j >> (2 - a)) & 1) - ((i >> (2 - a)) & 1);
-          if (std::max(std::abs(o[0]), std::max(std::abs(o[1]), std::abs(o[2]))) > 1)
-            tab[d * 64 + i * 8 + j] = (short)compact[offset_index(o[0], o[1], o[2])];
-        }
-    m2l_set_pair_table(tab.data(), nullptr);
     KCHECK(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, E.device));
     // one work item per target parent of a node with a V list
     std::vector<int> qlist;
@@ -435,16 +438,14 @@ struct Impl : ImplBase {
     args.tval = tval;
   }
 
-  void gemm(int M, int K, const double* A, const T* B, int64_t ldb, const int* bidx, T* C, int64_t ldc, const int* cidx,
-            int ncol, bool acc, int out_lvl, bool in_on, int in_lvl, cudaStream_t st) {
+  // col_lvl set: output rows scaled by 2^(-(depth + rootlvl) * deg)
+  void gemm(int M, int K, const T* A, const T* B, int64_t ldb, const int* bidx, T* C, int64_t ldc, const int* cidx,
+            int ncol, bool acc, cudaStream_t st, const int* col_lvl = nullptr) {
     if (ncol <= 0) return;
     GemmScale s = scl;
-    s.out_on = 1;
-    s.out_lvl = out_lvl;
-    s.in_on = in_on ? 1 : 0;
-    s.in_lvl = in_lvl;
-    launch_node_gemm<T>(M, K, A, B, ldb, bidx, C, ldc, cidx, ncol, acc, s, st);
-    nlaunch++;
+    s.col_lvl = col_lvl;
+    s.lvl_base = E.rootlvl;
+    nlaunch += launch_node_gemm<T>(M, K, A, B, ldb, bidx, C, ldc, cidx, ncol, acc, s, gemm_ws, gemm_ws_len, num_sms, st);
   }
 
   void p2p(const List& l, int which, int rhs, cudaStream_t st) {
@@ -463,7 +464,7 @@ struct Impl : ImplBase {
   int eval(const double* d_srcden, double* d_trgval, int nrhs, cudaStream_t st) override {
     ensure_rhs(nrhs);
     nlaunch = 0;
-    const int md = tr.maxdepth, rl = E.rootlvl;
+    const int md = tr.maxdepth;
     const int K1 = nsurf * sd_m;
     bool prof = E.profiling;
     if (prof) KCHECK(cudaEventRecord(ev[0], st));
@@ -472,13 +473,14 @@ struct Impl : ImplBase {
     for (int r = 0; r < nrhs; r++) {
       // upward
       p2p(s2m, P2P_S2M, r, st);
-      for (int d = md; d >= 2; d--) {
-        const List& L = up_leaf[d];
-        gemm(K1, nuc * td_m, A_uc2ue, supcval, (int64_t)nuc * td_m, L.work, supeden, K1, L.work, L.n, false, d + rl,
-             false, 0, st);
+      // y = up_W * check on the leaves of every level at once, M2M bottom-up
+      // in y coordinates, then every node's density = 2^(-l deg) up_V * y
+      gemm(ru, nuc * td_m, A_upW, supcval, (int64_t)nuc * td_m, s2m.work, ybuf, ru, s2m.work, s2m.n, false, st);
+      for (int d = md - 1; d >= 2; d--) {
         const List& P = up_non[d];
-        gemm(K1, 8 * K1, A_m2m, supeden, K1, P.aux, supeden, K1, P.work, P.n, false, d + rl, true, d + 1 + rl, st);
+        gemm(ru, 8 * ru, A_m2my, ybuf, ru, P.aux, ybuf, ru, P.work, P.n, false, st);
       }
+      gemm(K1, ru, A_upV, ybuf, ru, up_all.work, supeden, K1, up_all.work, up_all.n, false, st, up_all.aux);
       if (prof && r == 0) KCHECK(cudaEventRecord(ev[1], st));
       // V list
       KCHECK(cudaMemsetAsync(tdncval, 0, sizeof(T) * (size_t)tr.nnodes * nsurf * td_m, st));
@@ -486,7 +488,7 @@ struct Impl : ImplBase {
         launch_m2l_forward<T>(geom, supeden, fwd.work, fwd.n, d_depth, spectra, st);
         if (prof && r == 0) KCHECK(cudaEventRecord(ev[7], st));
         if (pairs_n > 0)
-          launch_m2l_hadamard_pairs<T>(op.nfreq, khat, spectra, pairs_n, pairs_chd, pairs_coll, pairs_mask, effval,
+          launch_m2l_hadamard_sweep<T>(op.nfreq, khat, spectra, pairs_n, pairs_chd, pairs_coll, pairs_mask, effval,
                                        num_sms, st);
         else
           launch_m2l_hadamard<T>(geom, khat, spectra, m2l.work, m2l.n, m2l.ptr, m2l.idx, d_path, effval, st);
@@ -499,13 +501,16 @@ struct Impl : ImplBase {
       p2p(s2l, P2P_S2L, r, st);
       if (prof && r == 0) KCHECK(cudaEventRecord(ev[3], st));
       // downward
-      for (int d = 2; d <= md; d++) {
-        const List& L = dn[d];
-        gemm(K1, nsurf * td_m, A_dc2de, tdncval, (int64_t)nsurf * td_m, L.work, tdneden, K1, L.work, L.n, false, d + rl,
-             false, 0, st);
+      // z = dn_W * check on the target nodes of every level at once, L2L
+      // top-down in z coordinates into the 8 children, then every node's
+      // density = 2^(-l deg) dn_V * z
+      gemm(rd, nsurf * td_m, A_dnW, tdncval, (int64_t)nsurf * td_m, dn_all.work, zbuf, rd, dn_all.work, dn_all.n, false,
+           st);
+      for (int d = 3; d <= md; d++) {
         const List& P = dn_par[d];
-        gemm(8 * K1, K1, A_l2l, tdneden, K1, P.work, tdneden, K1, P.aux, P.n, true, d + rl, true, d - 1 + rl, st);
+        gemm(8 * rd, rd, A_l2lz, zbuf, rd, P.work, zbuf, rd, P.aux, P.n, true, st);
       }
+      gemm(K1, rd, A_dnV, zbuf, rd, dn_all.work, tdneden, K1, dn_all.work, dn_all.n, false, st, dn_all.aux);
       if (prof && r == 0) KCHECK(cudaEventRecord(ev[4], st));
       // leaves
       p2p(leaf, P2P_LEAF, r, st);
@@ -536,6 +541,8 @@ struct Impl : ImplBase {
     KCHECK(cudaGetLastError());
     return KIFMM_OK;
   }
+
+  void reserve(int nrhs) override { ensure_rhs(nrhs); }
 
   void phase_times(double* ms) const override {
     for (int i = 0; i < 9; i++) ms[i] = pt[i];
@@ -691,6 +698,42 @@ int Engine::eval_device(const double* d_srcden, double* d_trgval, int nrhs, cuda
     return KIFMM_ERR_CUDA;
   }
   return KIFMM_OK;
+}
+
+int Engine::reserve(int nrhs) {
+  if (!ready) {
+    err = "eval before a successful setup";
+    return KIFMM_ERR_STATE;
+  }
+  try {
+    impl->reserve(nrhs);
+  } catch (const CudaError& e) {
+    err = std::string(e.where) + ": " + cudaGetErrorString(e.e);
+    return KIFMM_ERR_CUDA;
+  }
+  return KIFMM_OK;
+}
+
+int Engine::enqueue(const double* d_srcden, double* d_trgval, int nrhs, cudaStream_t st) {
+  if (!ready) {
+    err = "eval before a successful setup";
+    return KIFMM_ERR_STATE;
+  }
+  if (nrhs < 1 || (!d_srcden && ns > 0) || (!d_trgval && nt > 0)) {
+    err = "bad eval arguments";
+    return KIFMM_ERR_ARG;
+  }
+  bool prof = profiling;
+  profiling = false;  // per-phase event timing synchronises; not inside a capture
+  int rc = KIFMM_OK;
+  try {
+    rc = impl->eval(d_srcden, d_trgval, nrhs, st);
+  } catch (const CudaError& e) {
+    err = std::string(e.where) + ": " + cudaGetErrorString(e.e);
+    rc = KIFMM_ERR_CUDA;
+  }
+  profiling = prof;
+  return rc;
 }
 
 int Engine::eval_host(const double* srcden, double* trgval, int nrhs) {

@@ -17,6 +17,8 @@ struct ImplBase {
   virtual ~ImplBase() = default;
   // device-resident densities/potentials (double, original point order)
   virtual int eval(const double* d_srcden, double* d_trgval, int nrhs, cudaStream_t st) = 0;
+  // grows the per-rhs buffers (no allocation may happen inside a stream capture)
+  virtual void reserve(int nrhs) = 0;
   virtual void phase_times(double* ms) const = 0;
   virtual int launches() const = 0;
 };
@@ -59,9 +61,18 @@ struct Engine {
   int setup();  // returns a kifmm_status
   int eval_host(const double* srcden, double* trgval, int nrhs);
   int eval_device(const double* d_srcden, double* d_trgval, int nrhs, cudaStream_t st, bool sync);
+  // Enqueues the evaluation passes on st without any host synchronisation
+  // or error query (usable inside a stream capture).
+  int enqueue(const double* d_srcden, double* d_trgval, int nrhs, cudaStream_t st);
+  int reserve(int nrhs);
   int direct(const double* srcden, int nt_chk, const double* tpos, double* out);
   int check(const double* srcden, const double* trgval, int numchk, uint64_t seed, double* relerr);
   void release_device();
 };
 
 }  // namespace kifmm
+
+// The opaque handle of the C ABI (kifmm_handle in kifmm.h).
+struct kifmm_engine {
+  kifmm::Engine e;
+};

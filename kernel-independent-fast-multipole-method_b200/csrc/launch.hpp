@@ -56,16 +56,23 @@ void launch_gather_val(const T* tval, const int* perm, int nt, int td, int nrhs,
 //   C[cidx[j]*ldc + r] (=|+=) rs(r) * sum_k A[r*K + k] * ks(k) * B[bidx[j]*ldb + k]
 // with rs(r) = 2^(-out_lvl*deg[r % sd]) and ks(k) = 2^(in_lvl*deg[k % sd])
 // when the respective scaling is enabled.  A is M x K row-major.
+// When col_lvl is set, column j uses out level col_lvl[j] + lvl_base instead
+// of out_lvl (one launch then covers nodes of every level).
+// Output row r of column j is multiplied by 2^(-(col_lvl[j] + lvl_base) *
+// deg[r % sd]) when col_lvl is set (homogeneous level scaling).
 struct GemmScale {
   int sd = 1;
   int deg[4] = {0, 0, 0, 0};
-  int out_on = 0, out_lvl = 0;
-  int in_on = 0, in_lvl = 0;
+  const int* col_lvl = nullptr;
+  int lvl_base = 0;
 };
 
+// ws (FP64, ws_len doubles) lets a launch with few columns split K over
+// several CTAs; pass nullptr to disable.
 template <typename T>
-void launch_node_gemm(int M, int K, const double* A, const T* B, int64_t ldb, const int* bidx, T* C, int64_t ldc,
-                      const int* cidx, int ncol, bool accumulate, const GemmScale& sc, cudaStream_t st);
+int launch_node_gemm(int M, int K, const T* A, const T* B, int64_t ldb, const int* bidx, T* C, int64_t ldc,
+                      const int* cidx, int ncol, bool accumulate, const GemmScale& sc, double* ws, size_t ws_len,
+                      int num_sms, cudaStream_t st);
 
 // FFT-based M2L (MatMgnt3d::plnden2effden / UE2DC_dgemv / effval2plnval,
 // fmm3d/matmgnt3d.cpp:223-361).
@@ -86,11 +93,11 @@ template <typename T>
 void launch_m2l_hadamard(const M2LGeom& g, const T* khat, const T* spectra, const int* work, int nwork,
                          const int64_t* vptr, const int* vidx, const int* path, T* effval, cudaStream_t st);
 // Parent-pair form for single-dof kernels: effval[child of Q] for the nq target
-// parents, operator spectra in compact [316][nfreq] order (see m2l.cu).
+// parents Q (first child qchd[q], colleague first children coll[q][26], -1 when
+// absent, V-list children mask[q]); operator spectra [343][nfreq] (m2l.cu).
 template <typename T>
-void launch_m2l_hadamard_pairs(int nf, const T* khat_c, const T* spectra, int nq, const int* qchd, const int* coll,
+void launch_m2l_hadamard_sweep(int nf, const T* khat_c, const T* spectra, int nq, const int* qchd, const int* coll,
                                const unsigned char* mask, T* effval, int num_sms, cudaStream_t st);
-void m2l_set_pair_table(const short* tab, cudaStream_t st);
 // tdncval[node] += extract(inverse(effval[node]))
 template <typename T>
 void launch_m2l_inverse(const M2LGeom& g, const T* effval, const int* work, int nwork, T* tdncval,

@@ -22,94 +22,173 @@ namespace kifmm {
 namespace {
 
 constexpr int FFT_THREADS = 256;
-constexpr int NPMAX = 8, NMAX = 16, NHMAX = 9;
 
 template <typename T>
 struct Cpx {
   T re, im;
 };
 
+// ---------------------------------------------------------------------------
+// Warp-per-node transforms.  One warp carries one node through all passes
+// with only warp-level synchronisation, so a CTA keeps up to 8 nodes in
+// flight and never waits on a CTA-wide barrier between passes.  Shared
+// memory: the CTA's twiddle-product table W2[n*n], then one region per warp.
 template <typename T>
-__device__ __forceinline__ void twiddles(Cpx<T>* w, int n) {
-  for (int m = threadIdx.x; m < n; m += blockDim.x) {
+__device__ __forceinline__ void fill_w2(Cpx<T>* W2, int n) {
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+    int m = ((e / n) * (e % n)) % n;
     double s, c;
     sincospi(-2.0 * (double)m / (double)n, &s, &c);
-    w[m].re = (T)c;
-    w[m].im = (T)s;
+    W2[e].re = (T)c;
+    W2[e].im = (T)s;
   }
 }
 
-// spectra[node][s][f], f = (kz*n + ky)*nh + kx
+__host__ __device__ inline size_t align16(size_t b) { return (b + 15) & ~(size_t)15; }
+
 template <typename T>
-__global__ void __launch_bounds__(FFT_THREADS) k_m2l_fwd(M2LGeom g, const T* __restrict__ supeden,
-                                                          const int* __restrict__ nodes, int nwork,
-                                                          const int* __restrict__ depth, T* __restrict__ spectra) {
-  __shared__ T xg[NPMAX * NPMAX * NPMAX];
-  __shared__ Cpx<T> A[NPMAX * NPMAX * NHMAX];  // A[k][j][kx]
-  __shared__ Cpx<T> Bm[NPMAX * NMAX * NHMAX];  // B[k][ky][kx]
-  __shared__ Cpx<T> w[NMAX];
-  __shared__ Cpx<T> W2[NMAX * NMAX];  // W2[a*n + b] = w^(a*b mod n)
+__host__ __device__ inline size_t fwd_warp_bytes(int np, int n, int nh) {
+  return align16(sizeof(T) * np * np * np) + align16(sizeof(Cpx<T>) * np * np * nh) +
+         align16(sizeof(Cpx<T>) * np * n * nh);
+}
+
+template <typename T>
+__host__ __device__ inline size_t inv_warp_bytes(int np, int n, int nh) {
+  return align16(sizeof(Cpx<T>) * n * n * nh) + align16(sizeof(Cpx<T>) * np * n * nh) +
+         align16(sizeof(Cpx<T>) * np * np * nh);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_m2l_fwd_warp(M2LGeom g, const T* __restrict__ supeden,
+                                                      const int* __restrict__ nodes, int nwork,
+                                                      const int* __restrict__ depth, T* __restrict__ spectra) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   const int np = g.np, n = g.n, nh = g.nh, nf = g.nfreq;
-  twiddles(w, n);
+  Cpx<T>* W2 = reinterpret_cast<Cpx<T>*>(smem_raw);
+  fill_w2(W2, n);
   __syncthreads();
-  for (int e = threadIdx.x; e < n * n; e += blockDim.x) W2[e] = w[((e / n) * (e % n)) % n];
-  for (int wi = blockIdx.x; wi < nwork; wi += gridDim.x) {
-  const int node = nodes[wi];
-  const int lvl = depth[node] + g.rootlvl;
-  const T* den = supeden + (size_t)node * g.nsurf * g.sd;
-  for (int s = 0; s < g.sd; s++) {
-    T scale = (T)ldexp(1.0, lvl * g.deg[s]);  // plnden2effden scaling, matmgnt3d.cpp:228-235
-    for (int e = threadIdx.x; e < np * np * np; e += blockDim.x) xg[e] = T(0);
-    __syncthreads();
-    for (int k = threadIdx.x; k < g.nsurf; k += blockDim.x) {
-      int i = g.surf_ijk[3 * k], j = g.surf_ijk[3 * k + 1], kk = g.surf_ijk[3 * k + 2];
-      xg[(i * np + j) * np + kk] = den[(size_t)k * g.sd + s] * scale;
-    }
-    __syncthreads();
-    // x pass: A[k][j][kx] = sum_i x[i][j][k] w^(i kx)
-    for (int e = threadIdx.x; e < np * np * nh; e += blockDim.x) {
-      int kx = e % nh, j = (e / nh) % np, k = e / (nh * np);
-      T re = 0, im = 0;
-      for (int i = 0; i < np; i++) {
-        T v = xg[(i * np + j) * np + k];
-        Cpx<T> t = W2[i * n + kx];
-        re += v * t.re;
-        im += v * t.im;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpc = blockDim.x >> 5;
+  unsigned char* mine = smem_raw + align16(sizeof(Cpx<T>) * n * n) + (size_t)warp * fwd_warp_bytes<T>(np, n, nh);
+  T* xg = reinterpret_cast<T*>(mine);
+  Cpx<T>* A = reinterpret_cast<Cpx<T>*>(mine + align16(sizeof(T) * np * np * np));
+  Cpx<T>* Bm = reinterpret_cast<Cpx<T>*>(reinterpret_cast<unsigned char*>(A) + align16(sizeof(Cpx<T>) * np * np * nh));
+  for (int wi = blockIdx.x * wpc + warp; wi < nwork; wi += gridDim.x * wpc) {
+    const int node = nodes[wi];
+    const int lvl = depth[node] + g.rootlvl;
+    const T* den = supeden + (size_t)node * g.nsurf * g.sd;
+    for (int s = 0; s < g.sd; s++) {
+      const T scale = (T)ldexp(1.0, lvl * g.deg[s]);  // plnden2effden scaling, matmgnt3d.cpp:228-235
+      for (int e = lane; e < np * np * np; e += 32) xg[e] = T(0);
+      __syncwarp();
+      for (int k = lane; k < g.nsurf; k += 32) {
+        int i = g.surf_ijk[3 * k], j = g.surf_ijk[3 * k + 1], kk = g.surf_ijk[3 * k + 2];
+        xg[(i * np + j) * np + kk] = den[(size_t)k * g.sd + s] * scale;
       }
-      A[e].re = re;
-      A[e].im = im;
-    }
-    __syncthreads();
-    // y pass: B[k][ky][kx] = sum_j A[k][j][kx] w^(j ky)
-    for (int e = threadIdx.x; e < np * n * nh; e += blockDim.x) {
-      int kx = e % nh, ky = (e / nh) % n, k = e / (nh * n);
-      T re = 0, im = 0;
-      for (int j = 0; j < np; j++) {
-        Cpx<T> a = A[(k * np + j) * nh + kx];
-        Cpx<T> t = W2[j * n + ky];
-        re += a.re * t.re - a.im * t.im;
-        im += a.re * t.im + a.im * t.re;
+      __syncwarp();
+      for (int e = lane; e < np * np * nh; e += 32) {  // x pass
+        int kx = e % nh, j = (e / nh) % np, k = e / (nh * np);
+        T re = 0, im = 0;
+        for (int i = 0; i < np; i++) {
+          T v = xg[(i * np + j) * np + k];
+          Cpx<T> t = W2[i * n + kx];
+          re += v * t.re;
+          im += v * t.im;
+        }
+        A[e].re = re;
+        A[e].im = im;
       }
-      Bm[e].re = re;
-      Bm[e].im = im;
-    }
-    __syncthreads();
-    // z pass: out[kz][ky][kx] = sum_k B[k][ky][kx] w^(k kz)
-    T* out = spectra + ((size_t)node * g.sd + s) * nf * 2;
-    for (int e = threadIdx.x; e < nf; e += blockDim.x) {
-      int kxy = e % (n * nh), kz = e / (n * nh);
-      T re = 0, im = 0;
-      for (int k = 0; k < np; k++) {
-        Cpx<T> b = Bm[k * n * nh + kxy];
-        Cpx<T> t = W2[k * n + kz];
-        re += b.re * t.re - b.im * t.im;
-        im += b.re * t.im + b.im * t.re;
+      __syncwarp();
+      for (int e = lane; e < np * n * nh; e += 32) {  // y pass
+        int kx = e % nh, ky = (e / nh) % n, k = e / (nh * n);
+        T re = 0, im = 0;
+        for (int j = 0; j < np; j++) {
+          Cpx<T> a = A[(k * np + j) * nh + kx];
+          Cpx<T> t = W2[j * n + ky];
+          re += a.re * t.re - a.im * t.im;
+          im += a.re * t.im + a.im * t.re;
+        }
+        Bm[e].re = re;
+        Bm[e].im = im;
       }
-      out[2 * e] = re;
-      out[2 * e + 1] = im;
+      __syncwarp();
+      Cpx<T>* out = reinterpret_cast<Cpx<T>*>(spectra + ((size_t)node * g.sd + s) * nf * 2);
+      for (int e = lane; e < nf; e += 32) {  // z pass
+        int kxy = e % (n * nh), kz = e / (n * nh);
+        Cpx<T> r;
+        r.re = r.im = T(0);
+        for (int k = 0; k < np; k++) {
+          Cpx<T> b = Bm[k * n * nh + kxy];
+          Cpx<T> t = W2[k * n + kz];
+          r.re += b.re * t.re - b.im * t.im;
+          r.im += b.re * t.im + b.im * t.re;
+        }
+        out[e] = r;
+      }
+      __syncwarp();
     }
-    __syncthreads();
   }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_m2l_inv_warp(M2LGeom g, const T* __restrict__ effval,
+                                                      const int* __restrict__ work, int nwork,
+                                                      T* __restrict__ tdncval) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int np = g.np, n = g.n, nh = g.nh, nf = g.nfreq;
+  Cpx<T>* W2 = reinterpret_cast<Cpx<T>*>(smem_raw);
+  fill_w2(W2, n);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpc = blockDim.x >> 5;
+  unsigned char* mine = smem_raw + align16(sizeof(Cpx<T>) * n * n) + (size_t)warp * inv_warp_bytes<T>(np, n, nh);
+  Cpx<T>* Y = reinterpret_cast<Cpx<T>*>(mine);
+  Cpx<T>* Bm = reinterpret_cast<Cpx<T>*>(mine + align16(sizeof(Cpx<T>) * n * n * nh));
+  Cpx<T>* A = reinterpret_cast<Cpx<T>*>(reinterpret_cast<unsigned char*>(Bm) + align16(sizeof(Cpx<T>) * np * n * nh));
+  for (int wi = blockIdx.x * wpc + warp; wi < nwork; wi += gridDim.x * wpc) {
+    const int node = work[wi];
+    T* dst = tdncval + (size_t)node * g.nsurf * g.td;
+    for (int t = 0; t < g.td; t++) {
+      const Cpx<T>* src = reinterpret_cast<const Cpx<T>*>(effval + ((size_t)node * g.td + t) * nf * 2);
+      for (int e = lane; e < nf; e += 32) Y[e] = src[e];
+      __syncwarp();
+      for (int e = lane; e < np * n * nh; e += 32) {  // z pass (inverse), k < np
+        int kxy = e % (n * nh), k = e / (n * nh);
+        T re = 0, im = 0;
+        for (int kz = 0; kz < n; kz++) {
+          Cpx<T> y = Y[kz * n * nh + kxy];
+          Cpx<T> c = W2[k * n + kz];
+          re += y.re * c.re + y.im * c.im;
+          im += y.im * c.re - y.re * c.im;
+        }
+        Bm[e].re = re;
+        Bm[e].im = im;
+      }
+      __syncwarp();
+      for (int e = lane; e < np * np * nh; e += 32) {  // y pass (inverse), j < np
+        int kx = e % nh, j = (e / nh) % np, k = e / (nh * np);
+        T re = 0, im = 0;
+        for (int ky = 0; ky < n; ky++) {
+          Cpx<T> b = Bm[(k * n + ky) * nh + kx];
+          Cpx<T> c = W2[j * n + ky];
+          re += b.re * c.re + b.im * c.im;
+          im += b.im * c.re - b.re * c.im;
+        }
+        A[e].re = re;
+        A[e].im = im;
+      }
+      __syncwarp();
+      for (int m = lane; m < g.nsurf; m += 32) {  // c2r along x at the surface points
+        int i = g.surf_ijk[3 * m], j = g.surf_ijk[3 * m + 1], k = g.surf_ijk[3 * m + 2];
+        const Cpx<T>* a = &A[(k * np + j) * nh];
+        T v = a[0].re + ((i & 1) ? -a[nh - 1].re : a[nh - 1].re);
+        T acc = 0;
+        for (int kx = 1; kx < nh - 1; kx++) {
+          Cpx<T> c = W2[i * n + kx];
+          acc += a[kx].re * c.re + a[kx].im * c.im;
+        }
+        dst[(size_t)m * g.td + t] += v + T(2) * acc;
+      }
+      __syncwarp();
+    }
   }
 }
 
@@ -170,186 +249,20 @@ __global__ void __launch_bounds__(FFT_THREADS) k_m2l_had(M2LGeom g, const T* __r
   }
 }
 
-// ---------------------------------------------------------------------------
-// Hadamard accumulation in parent-pair form (single-dof equivalent kernel).
-//
-// The V list of a node t is the set of children c of the 26 colleagues P of
-// t's parent Q that are not adjacent to t (fmm3d/let3d.cpp:228-247), and the
-// translation from c to t depends only on the offset 2*(P-Q) + oct(c) -
-// oct(t), one of 316 values.  So per frequency the whole pass is, for every
-// target parent Q, Y[Q's 8 children] += sum_dir M_dir * X[P_dir's 8 children]
-// with 8x8 blocks drawn from the same 316 operator values.
-//
-// One CTA owns a tile of 32 frequencies (one per lane) for a slice of the
-// target parents; the 316 operator spectra of that tile sit in shared memory
-// for the CTA's whole lifetime.  A warp accumulates the 8 children of QPT
-// parents at once in registers, so each operator value read from shared
-// memory feeds QPT complex multiply-adds and each source spectrum read from
-// global memory feeds up to 8.
-__constant__ short c_pair_off[26 * 64];  // [dir][i][j] -> compact offset index, -1 when adjacent
-
-template <typename T, int QPT>
-__global__ void __launch_bounds__(256) k_m2l_had_pairs(int nf, const T* __restrict__ khat_c,
-                                                       const T* __restrict__ spectra, int nq,
-                                                       const int* __restrict__ qchd, const int* __restrict__ coll,
-                                                       const unsigned char* __restrict__ mask,
-                                                       T* __restrict__ effval) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  Cpx<T>* Ks = reinterpret_cast<Cpx<T>*>(smem_raw);  // [316][32]
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int f0 = blockIdx.x * 32;
-  const int f = f0 + lane;
-  const bool fv = f < nf;
-  for (int e = threadIdx.x; e < 316 * 32; e += blockDim.x) {
-    int o = e >> 5, l = e & 31;
-    Cpx<T> v;
-    v.re = v.im = T(0);
-    if (f0 + l < nf) {
-      v.re = khat_c[((size_t)o * nf + f0 + l) * 2];
-      v.im = khat_c[((size_t)o * nf + f0 + l) * 2 + 1];
-    }
-    Ks[e] = v;
-  }
-  __syncthreads();
-  const int nwarps_total = gridDim.y * (blockDim.x >> 5);
-  const int gw = blockIdx.y * (blockDim.x >> 5) + warp;
-  for (int q0 = gw * QPT; q0 < nq; q0 += nwarps_total * QPT) {
-    T ar[QPT][8], ai[QPT][8];
-#pragma unroll
-    for (int q = 0; q < QPT; q++)
-#pragma unroll
-      for (int i = 0; i < 8; i++) ar[q][i] = ai[q][i] = T(0);
-    for (int dir = 0; dir < 26; dir++) {
-      int base[QPT];
-      bool any = false;
-#pragma unroll
-      for (int q = 0; q < QPT; q++) {
-        base[q] = (q0 + q < nq) ? coll[(size_t)(q0 + q) * 26 + dir] : -1;
-        any |= base[q] >= 0;
-      }
-      if (!any) continue;
-      const short* offs = &c_pair_off[dir * 64];
-#pragma unroll
-      for (int j = 0; j < 8; j++) {
-        T xr[QPT], xi[QPT];
-#pragma unroll
-        for (int q = 0; q < QPT; q++) {
-          xr[q] = xi[q] = T(0);
-          if (base[q] >= 0 && fv) {
-            const T* X = spectra + ((size_t)(base[q] + j) * nf + f) * 2;
-            xr[q] = X[0];
-            xi[q] = X[1];
-          }
-        }
-#pragma unroll
-        for (int i = 0; i < 8; i++) {
-          int o = offs[i * 8 + j];
-          if (o < 0) continue;
-          Cpx<T> k = Ks[o * 32 + lane];
-#pragma unroll
-          for (int q = 0; q < QPT; q++) {
-            ar[q][i] += k.re * xr[q] - k.im * xi[q];
-            ai[q][i] += k.re * xi[q] + k.im * xr[q];
-          }
-        }
-      }
-    }
-    if (fv) {
-#pragma unroll
-      for (int q = 0; q < QPT; q++) {
-        if (q0 + q >= nq) continue;
-        int c0 = qchd[q0 + q];
-        unsigned m = mask[q0 + q];
-#pragma unroll
-        for (int i = 0; i < 8; i++) {
-          if (!((m >> i) & 1)) continue;
-          T* Y = effval + ((size_t)(c0 + i) * nf + f) * 2;
-          Y[0] = ar[q][i];
-          Y[1] = ai[q][i];
-        }
-      }
-    }
-  }
-}
-
-// tdncval[node][m][t] += real inverse transform of effval at the surface points
-template <typename T>
-__global__ void __launch_bounds__(FFT_THREADS) k_m2l_inv(M2LGeom g, const T* __restrict__ effval,
-                                                          const int* __restrict__ work, int nwork,
-                                                          T* __restrict__ tdncval) {
-  // dynamic shared memory: Y[n*n*nh] | B[np*n*nh] | A[np*np*nh] | w[n]
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int np = g.np, n = g.n, nh = g.nh, nf = g.nfreq;
-  Cpx<T>* Y = reinterpret_cast<Cpx<T>*>(smem_raw);
-  Cpx<T>* Bm = Y + n * n * nh;
-  Cpx<T>* A = Bm + np * n * nh;
-  Cpx<T>* w = A + np * np * nh;
-  Cpx<T>* W2 = w + n;  // W2[a*n + b] = w^(a*b mod n)
-  twiddles(w, n);
-  __syncthreads();
-  for (int e = threadIdx.x; e < n * n; e += blockDim.x) W2[e] = w[((e / n) * (e % n)) % n];
-  for (int wi = blockIdx.x; wi < nwork; wi += gridDim.x) {
-  const int node = work[wi];
-  for (int t = 0; t < g.td; t++) {
-    const T* src = effval + ((size_t)node * g.td + t) * nf * 2;
-    for (int e = threadIdx.x; e < nf; e += blockDim.x) {
-      Y[e].re = src[2 * e];
-      Y[e].im = src[2 * e + 1];
-    }
-    __syncthreads();
-    // z pass (inverse): B[k][ky][kx] = sum_kz Y[kz][ky][kx] conj(w)^(k kz), k < np
-    for (int e = threadIdx.x; e < np * n * nh; e += blockDim.x) {
-      int kxy = e % (n * nh), k = e / (n * nh);
-      T re = 0, im = 0;
-      for (int kz = 0; kz < n; kz++) {
-        Cpx<T> y = Y[kz * n * nh + kxy];
-        Cpx<T> c = W2[k * n + kz];
-        re += y.re * c.re + y.im * c.im;
-        im += y.im * c.re - y.re * c.im;
-      }
-      Bm[e].re = re;
-      Bm[e].im = im;
-    }
-    __syncthreads();
-    // y pass (inverse): A[k][j][kx] = sum_ky B[k][ky][kx] conj(w)^(j ky), j < np
-    for (int e = threadIdx.x; e < np * np * nh; e += blockDim.x) {
-      int kx = e % nh, j = (e / nh) % np, k = e / (nh * np);
-      T re = 0, im = 0;
-      for (int ky = 0; ky < n; ky++) {
-        Cpx<T> b = Bm[(k * n + ky) * nh + kx];
-        Cpx<T> c = W2[j * n + ky];
-        re += b.re * c.re + b.im * c.im;
-        im += b.im * c.re - b.re * c.im;
-      }
-      A[e].re = re;
-      A[e].im = im;
-    }
-    __syncthreads();
-    // x pass (c2r, Hermitian half line) at the surface points only
-    T* dst = tdncval + (size_t)node * g.nsurf * g.td;
-    for (int m = threadIdx.x; m < g.nsurf; m += blockDim.x) {
-      int i = g.surf_ijk[3 * m], j = g.surf_ijk[3 * m + 1], k = g.surf_ijk[3 * m + 2];
-      const Cpx<T>* a = &A[(k * np + j) * nh];
-      T v = a[0].re + ((i & 1) ? -a[nh - 1].re : a[nh - 1].re);
-      T acc = 0;
-      for (int kx = 1; kx < nh - 1; kx++) {
-        Cpx<T> c = W2[i * n + kx];
-        acc += a[kx].re * c.re + a[kx].im * c.im;  // Re(a * conj(w)^(i kx))
-      }
-      dst[(size_t)m * g.td + t] += v + T(2) * acc;
-    }
-    __syncthreads();
-  }
-  }
-}
-
 }  // namespace
 
 template <typename T>
 void launch_m2l_forward(const M2LGeom& g, const T* supeden, const int* nodes, int nn, const int* depth, T* spectra,
                         cudaStream_t st) {
   if (nn <= 0) return;
-  k_m2l_fwd<T><<<std::min(nn, 148 * 16), FFT_THREADS, 0, st>>>(g, supeden, nodes, nn, depth, spectra);
+  // warp per node; as many warps per CTA (<= 8) as fit in ~200 KB of shared memory
+  const size_t per_warp = fwd_warp_bytes<T>(g.np, g.n, g.nh);
+  const size_t head = align16(sizeof(Cpx<T>) * g.n * g.n);
+  int wpc = (int)std::max<size_t>(1, std::min<size_t>(8, (200 * 1024 - head) / per_warp));
+  size_t smem = head + per_warp * wpc;
+  cudaFuncSetAttribute(k_m2l_fwd_warp<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int grid = std::max(1, std::min((nn + wpc - 1) / wpc, 148 * 8));
+  k_m2l_fwd_warp<T><<<grid, 32 * wpc, smem, st>>>(g, supeden, nodes, nn, depth, spectra);
 }
 
 template <typename T>
@@ -367,13 +280,26 @@ void launch_m2l_hadamard(const M2LGeom& g, const T* khat, const T* spectra, cons
 template <typename T>
 void launch_m2l_inverse(const M2LGeom& g, const T* effval, const int* work, int nwork, T* tdncval, cudaStream_t st) {
   if (nwork <= 0) return;
-  size_t smem = sizeof(Cpx<T>) * ((size_t)g.n * g.n * g.nh + (size_t)g.np * g.n * g.nh + (size_t)g.np * g.np * g.nh +
-                                  g.n + (size_t)g.n * g.n);
-  if (smem > 48 * 1024) cudaFuncSetAttribute(k_m2l_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_m2l_inv<T><<<std::min(nwork, 148 * 8), FFT_THREADS, smem, st>>>(g, effval, work, nwork, tdncval);
+  const size_t per_warp = inv_warp_bytes<T>(g.np, g.n, g.nh);
+  const size_t head = align16(sizeof(Cpx<T>) * g.n * g.n);
+  int wpc = (int)std::max<size_t>(1, std::min<size_t>(8, (200 * 1024 - head) / per_warp));
+  size_t smem = head + per_warp * wpc;
+  cudaFuncSetAttribute(k_m2l_inv_warp<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int grid = std::max(1, std::min((nwork + wpc - 1) / wpc, 148 * 8));
+  k_m2l_inv_warp<T><<<grid, 32 * wpc, smem, st>>>(g, effval, work, nwork, tdncval);
 }
 
-// Persistent form: each CTA owns a contiguous slice of target parents (Morton
+// ---------------------------------------------------------------------------
+// Hadamard accumulation in parent-pair form (single-dof equivalent kernel).
+//
+// The V list of a node t is the set of children c of the 26 colleagues P of
+// t's parent Q that are not adjacent to t (fmm3d/let3d.cpp:228-247), and the
+// translation from c to t depends only on the offset 2*(P-Q) + oct(c) -
+// oct(t), one of 316 values.  So per frequency the whole pass is, for every
+// target parent Q, Y[Q's 8 children] += sum_dir M_dir * X[P_dir's 8 children]
+// with 8x8 blocks drawn from the same 316 operator values.
+//
+// Persistent sweep: each CTA owns a contiguous slice of target parents (Morton
 // order, so neighbouring parents share colleagues) and sweeps the frequency
 // tiles in order.  All CTAs therefore work on about the same tile at the same
 // time and its source spectra (nodes x 32 freq x 8 B, ~93 MB at 4M points)
@@ -505,7 +431,7 @@ __global__ void __launch_bounds__(NTHR) k_m2l_had_sweep(int nf, const T* __restr
 }
 
 template <typename T>
-void launch_m2l_hadamard_pairs(int nf, const T* khat, const T* spectra, int nq, const int* qchd, const int* coll,
+void launch_m2l_hadamard_sweep(int nf, const T* khat, const T* spectra, int nq, const int* qchd, const int* coll,
                                const unsigned char* mask, T* effval, int num_sms, cudaStream_t st) {
   if (nq <= 0) return;
   constexpr int QPT = 2;
@@ -517,12 +443,8 @@ void launch_m2l_hadamard_pairs(int nf, const T* khat, const T* spectra, int nq, 
   k_m2l_had_sweep<T, QPT, NTHR><<<grid, NTHR, smem, st>>>(nf, khat, spectra, nq, qchd, coll, mask, effval);
 }
 
-void m2l_set_pair_table(const short* tab, cudaStream_t st) {
-  cudaMemcpyToSymbolAsync(c_pair_off, tab, sizeof(short) * 26 * 64, 0, cudaMemcpyHostToDevice, st);
-}
-
 #define KIFMM_INST(T)                                                                                             \
-  template void launch_m2l_hadamard_pairs<T>(int, const T*, const T*, int, const int*, const int*,               \
+  template void launch_m2l_hadamard_sweep<T>(int, const T*, const T*, int, const int*, const int*,               \
                                              const unsigned char*, T*, int, cudaStream_t);                         \
   template void launch_m2l_forward<T>(const M2LGeom&, const T*, const int*, int, const int*, T*, cudaStream_t);  \
   template void launch_m2l_hadamard<T>(const M2LGeom&, const T*, const T*, const int*, int, const int64_t*,     \

@@ -1,6 +1,7 @@
 // Host FP64 precompute of the KIFMM translation operators; see operators.hpp.
 #include "operators.hpp"
 
+#include <algorithm>
 #include <barrier>
 #include <cmath>
 #include <map>
@@ -156,10 +157,16 @@ void surface_grid(int np, double R, std::vector<double>* pos, std::vector<int>* 
 // ---------------------------------------------------------------------------
 // One-sided Jacobi SVD (Hestenes) with round-robin parallel pair ordering.
 // ---------------------------------------------------------------------------
-bool pseudo_inverse(int m, int n, const double* a, double rel_cut, double* out, int nthreads) {
-  bool tr = m < n;
-  int R = tr ? n : m, C = tr ? m : n;  // B = tr ? A^T : A, R x C with R >= C
-  std::vector<double> U((size_t)R * C), V((size_t)C * C, 0.0);
+// On return B V = U with B = tr ? A^T : A (R x C, R >= C); the columns of U
+// (column-major, R per column) are orthogonal with norms sigma_c, V (C x C,
+// column-major) is orthogonal.
+static bool jacobi_svd(int m, int n, const double* a, int nthreads, bool& tr, int& R, int& C, std::vector<double>& U,
+                       std::vector<double>& V) {
+  tr = m < n;
+  R = tr ? n : m;
+  C = tr ? m : n;
+  U.assign((size_t)R * C, 0.0);
+  V.assign((size_t)C * C, 0.0);
   for (int c = 0; c < C; c++)
     for (int r = 0; r < R; r++) U[(size_t)c * R + r] = tr ? a[(size_t)c * n + r] : a[(size_t)r * n + c];
   for (int c = 0; c < C; c++) V[(size_t)c * C + c] = 1.0;
@@ -241,7 +248,50 @@ bool pseudo_inverse(int m, int n, const double* a, double rel_cut, double* out, 
   worker(0);
   for (auto& x : th) x.join();
   (void)sweep;
-  if (!converged) return false;
+  return converged;
+}
+
+bool pinv_factors(int m, int n, const double* a, double rel_cut, int nthreads, std::vector<double>* Vout,
+                  std::vector<double>* Wout, int* rank) {
+  bool tr;
+  int R, C;
+  std::vector<double> U, V;
+  if (!jacobi_svd(m, n, a, nthreads, tr, R, C, U, V)) return false;
+  std::vector<double> sig(C);
+  double smax = 0.0;
+  for (int c = 0; c < C; c++) {
+    double s = 0;
+    for (int r = 0; r < R; r++) s += U[(size_t)c * R + r] * U[(size_t)c * R + r];
+    sig[c] = std::sqrt(s);
+    smax = std::max(smax, sig[c]);
+  }
+  std::vector<int> keep;  // in decreasing singular value order
+  for (int c = 0; c < C; c++)
+    if (sig[c] >= rel_cut * smax && sig[c] > 0.0) keep.push_back(c);
+  std::sort(keep.begin(), keep.end(), [&](int x, int y) { return sig[x] > sig[y]; });
+  const int r = (int)keep.size();
+  // pinv(A) = sum_c (n-vector p_c)(m-vector q_c)^T with p_c unit length:
+  //   not transposed: p_c = V_c,          q_c = U_c / sigma_c^2
+  //   transposed:     p_c = U_c / sigma_c, q_c = V_c / sigma_c
+  Vout->assign((size_t)n * r, 0.0);
+  Wout->assign((size_t)r * m, 0.0);
+  for (int k = 0; k < r; k++) {
+    int c = keep[k];
+    const double* u = &U[(size_t)c * R];
+    const double* v = &V[(size_t)c * C];
+    double s = sig[c];
+    for (int j = 0; j < n; j++) (*Vout)[(size_t)j * r + k] = tr ? u[j] / s : v[j];
+    for (int i = 0; i < m; i++) (*Wout)[(size_t)k * m + i] = tr ? v[i] / s : u[i] / (s * s);
+  }
+  *rank = r;
+  return true;
+}
+
+bool pseudo_inverse(int m, int n, const double* a, double rel_cut, double* out, int nthreads) {
+  bool tr;
+  int R, C;
+  std::vector<double> U, V;
+  if (!jacobi_svd(m, n, a, nthreads, tr, R, C, U, V)) return false;
   // singular values, truncation (common/svdrep.cpp:51-58)
   std::vector<double> sig(C);
   double smax = 0.0;
@@ -324,43 +374,50 @@ std::shared_ptr<Operators> build_operators(const KernelDesc& mm, int np, int nth
   // UC2UE = pinv(K(UC <- UE)) at level 0 (fmm3d/matmgnt3d.cpp:96-105)
   std::vector<double> ue2ucm((size_t)nc * td * ns * sd);
   kernel_matrix(mm, nc, o.uc.data(), ns, o.ue.data(), o.ue.data(), ue2ucm.data());
-  o.uc2ue.resize((size_t)ns * sd * nc * td);
-  if (!pseudo_inverse(nc * td, ns * sd, ue2ucm.data(), cut, o.uc2ue.data(), nthreads)) {
+  if (!pinv_factors(nc * td, ns * sd, ue2ucm.data(), cut, nthreads, &o.up_V, &o.up_W, &o.rank_up)) {
     if (err) *err = "UC2UE SVD did not converge";
     return nullptr;
   }
   // DC2DE = pinv(K(DC <- DE)) (fmm3d/matmgnt3d.cpp:163-172)
   std::vector<double> de2dcm((size_t)ns * td * ns * sd);
   kernel_matrix(mm, ns, o.dc.data(), ns, o.de.data(), o.de.data(), de2dcm.data());
-  o.dc2de.resize((size_t)ns * sd * ns * td);
-  if (!pseudo_inverse(ns * td, ns * sd, de2dcm.data(), cut, o.dc2de.data(), nthreads)) {
+  if (!pinv_factors(ns * td, ns * sd, de2dcm.data(), cut, nthreads, &o.dn_V, &o.dn_W, &o.rank_dn)) {
     if (err) *err = "DC2DE SVD did not converge";
     return nullptr;
   }
-  // M2M_o = UC2UE * UE2UC_o, UE2UC_o: UE shifted by (2*idx-1), UC scaled x2 (:131-138)
+  // M2M_o = UC2UE * UE2UC_o, UE2UC_o: UE shifted by (2*idx-1), UC scaled x2
+  // (fmm3d/matmgnt3d.cpp:131-138).  With UC2UE = up_V * up_W the upward pass
+  // runs on y = up_W * (check values): a parent's y is sum_o (up_W UE2UC_o up_V)
+  // y_child_o; the child's 2^(-l deg) output and the parent's 2^(+l deg) input
+  // scaling cancel exactly.  Same for L2L_o = DC2DE * DE2DC_o, DE2DC_o: DC
+  // scaled x0.5 and shifted by (idx-0.5) (:199-203), on z = dn_W * (check values).
   const int K1 = ns * sd;
-  o.m2m.assign((size_t)K1 * 8 * K1, 0.0);
-  o.l2l.assign((size_t)8 * K1 * K1, 0.0);
+  const int ru = o.rank_up, rd = o.rank_dn;
+  o.m2m_y.assign((size_t)ru * 8 * ru, 0.0);
+  o.l2l_z.assign((size_t)8 * rd * rd, 0.0);
   parallel_range(8, nthreads, [&](int oct) {
     int idx[3] = {(oct >> 2) & 1, (oct >> 1) & 1, oct & 1};
     std::vector<double> chk(o.uc.size()), den(o.ue.size());
     for (size_t i = 0; i < o.uc.size(); i++) chk[i] = 2.0 * o.uc[i];
     for (int j = 0; j < ns; j++)
       for (int d = 0; d < 3; d++) den[3 * j + d] = o.ue[3 * j + d] + (2 * idx[d] - 1);
-    std::vector<double> ue2uc((size_t)nc * td * K1), prod((size_t)K1 * K1);
+    std::vector<double> ue2uc((size_t)nc * td * K1);
     kernel_matrix(mm, nc, chk.data(), ns, den.data(), den.data(), ue2uc.data());
-    matmul(K1, nc * td, K1, o.uc2ue.data(), ue2uc.data(), prod.data());
-    for (int r = 0; r < K1; r++)
-      for (int c = 0; c < K1; c++) o.m2m[(size_t)r * 8 * K1 + (size_t)oct * K1 + c] = prod[(size_t)r * K1 + c];
-    // L2L_o = DC2DE * DE2DC_o, DE2DC_o: DC scaled x0.5 and shifted by (idx-0.5) (:199-203)
+    std::vector<double> qb((size_t)ru * K1), qy((size_t)ru * ru);
+    matmul(ru, nc * td, K1, o.up_W.data(), ue2uc.data(), qb.data());
+    matmul(ru, K1, ru, qb.data(), o.up_V.data(), qy.data());
+    for (int r = 0; r < ru; r++)
+      for (int c = 0; c < ru; c++) o.m2m_y[(size_t)r * 8 * ru + (size_t)oct * ru + c] = qy[(size_t)r * ru + c];
     std::vector<double> dchk(o.dc.size());
     for (int j = 0; j < ns; j++)
       for (int d = 0; d < 3; d++) dchk[3 * j + d] = 0.5 * o.dc[3 * j + d] + (double(idx[d]) - 0.5);
     std::vector<double> de2dc((size_t)ns * td * K1);
     kernel_matrix(mm, ns, dchk.data(), ns, o.de.data(), o.de.data(), de2dc.data());
-    matmul(K1, ns * td, K1, o.dc2de.data(), de2dc.data(), prod.data());
-    for (int r = 0; r < K1; r++)
-      for (int c = 0; c < K1; c++) o.l2l[((size_t)oct * K1 + r) * K1 + c] = prod[(size_t)r * K1 + c];
+    std::vector<double> rb((size_t)rd * K1), rz((size_t)rd * rd);
+    matmul(rd, ns * td, K1, o.dn_W.data(), de2dc.data(), rb.data());
+    matmul(rd, K1, rd, rb.data(), o.dn_V.data(), rz.data());
+    for (int r = 0; r < rd; r++)
+      for (int c = 0; c < rd; c++) o.l2l_z[((size_t)oct * rd + r) * rd + c] = rz[(size_t)r * rd + c];
   });
 
   // M2L spectra (fmm3d/matmgnt3d.cpp:307-325): kernel sampled at

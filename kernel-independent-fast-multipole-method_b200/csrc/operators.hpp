@@ -8,10 +8,9 @@
 //   M2L spectra        FFT of the kernel sampled on the (2np)^3 grid,
 //                      fmm3d/matmgnt3d.cpp:296-361 (regposcal :400-420)
 //
-// The device passes use fused forms: M2M = UC2UE * [UE2UC_0 .. UE2UC_7] and
-// L2L = [DC2DE * DE2DC_0; ..; DC2DE * DE2DC_7]; the per-level homogeneous
-// scalings 2^(+-l*deg) (fmm3d/matmgnt3d.cpp:107-118,141-153) are applied in
-// the GEMM prologue/epilogue.
+// The device passes use the pseudo-inverses in factored form (see Operators);
+// the per-level homogeneous scalings 2^(+-l*deg) (fmm3d/matmgnt3d.cpp:107-118,
+// 141-153) are applied in the epilogue of the V-factor GEMMs.
 #pragma once
 
 #include <complex>
@@ -45,6 +44,10 @@ void kernel_matrix(const KernelDesc& k, int nt, const double* trg, int ns, const
 // common/svdrep.cpp:31-74).  a is m x n row-major; out is n x m row-major.
 // Returns false if the one-sided Jacobi SVD did not converge.
 bool pseudo_inverse(int m, int n, const double* a, double rel_cut, double* out, int nthreads);
+// Same truncated SVD, returned as factors pinv = V * W: V is n x r with
+// orthonormal columns, W = Sigma^-1 U^T is r x m (both row-major).
+bool pinv_factors(int m, int n, const double* a, double rel_cut, int nthreads, std::vector<double>* V,
+                  std::vector<double>* W, int* rank);
 
 struct Operators {
   KernelDesc mm;
@@ -56,11 +59,20 @@ struct Operators {
   std::vector<int> deg;   // per sd
   std::vector<double> ue, uc, de, dc;   // unit grids (3 per point), radii 1, 3, 3, 1
   std::vector<int> surf_ijk;            // (i,j,k) grid index of each np-surface point
-  std::vector<double> uc2ue;            // (nsurf*sd) x (nuc*td)
-  std::vector<double> m2m;              // (nsurf*sd) x (8*nsurf*sd)
-  std::vector<double> dc2de;            // (nsurf*sd) x (nsurf*td)
-  std::vector<double> l2l;              // (8*nsurf*sd) x (nsurf*sd)
   std::vector<std::complex<double>> m2l;  // [343 offsets][td][sd][nfreq], scaled by 1/n^3
+  // Surface contractions in factored form.  UC2UE = pinv(K(UC <- UE)) =
+  // up_V * up_W and DC2DE = pinv(K(DC <- DE)) = dn_V * dn_W, V with orthonormal
+  // columns and W = Sigma^-1 U^T.  The pseudo-inverses' entries reach
+  // 10^(np+1) times the data; applied as the two well-conditioned factors the
+  // products stay accurate in FP32, and the M2M / L2L chains run in the
+  // rank-r coordinates y = up_W * check and z = dn_W * check.
+  int rank_up = 0, rank_dn = 0;
+  std::vector<double> up_W;    // rank_up x (nuc*td)
+  std::vector<double> up_V;    // (nsurf*sd) x rank_up
+  std::vector<double> m2m_y;   // rank_up x (8*rank_up): block o = up_W * UE2UC_o * up_V
+  std::vector<double> dn_W;    // rank_dn x (nsurf*td)
+  std::vector<double> dn_V;    // (nsurf*sd) x rank_dn
+  std::vector<double> l2l_z;   // (8*rank_dn) x rank_dn: row block o = dn_W * DE2DC_o * dn_V
 };
 
 // Builds (or returns the cached) operators; nullptr + err on failure.

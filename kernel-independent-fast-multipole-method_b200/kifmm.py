@@ -62,6 +62,11 @@ SIGNATURES = {
     "kifmm_set_profiling": [_H, ctypes.c_int],
     "kifmm_work_counters": [_H, _DP, _IP],
     "kifmm_last_launch_count": [_H, _IP],
+    "kifmm_batch_create": [ctypes.c_int, ctypes.POINTER(_H), ctypes.POINTER(ctypes.c_void_p)],
+    "kifmm_batch_destroy": [ctypes.c_void_p],
+    "kifmm_batch_eval_device": [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
+                                ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p, ctypes.c_int],
+    "kifmm_batch_last_error": [ctypes.c_void_p],
     "kifmm_status_string": [ctypes.c_int],
     "kifmm_last_error": [_H],
 }
@@ -79,7 +84,8 @@ def lib():
         for name, argt in SIGNATURES.items():
             f = getattr(L, name)
             f.argtypes = argt
-            f.restype = ctypes.c_char_p if name in ("kifmm_status_string", "kifmm_last_error") else ctypes.c_int
+            f.restype = (ctypes.c_char_p if name in ("kifmm_status_string", "kifmm_last_error", "kifmm_batch_last_error")
+                         else ctypes.c_int)
         _lib = L
     return _lib
 
@@ -265,6 +271,35 @@ class FMM3d:
         n = ctypes.c_int()
         self._check(lib().kifmm_last_launch_count(self._h, ctypes.byref(n)))
         return n.value
+
+
+class Batch:
+    """Many set-up FMM3d instances evaluated together in one CUDA graph
+    (kifmm_batch_*): eval(srcden_ptrs, trgval_ptrs, nrhs, stream) takes one
+    device pointer pair per instance."""
+
+    def __init__(self, fmms):
+        self.fmms = list(fmms)
+        hs = (_H * len(self.fmms))(*[f._h for f in self.fmms])
+        self._b = ctypes.c_void_p()
+        st = lib().kifmm_batch_create(len(self.fmms), hs, ctypes.byref(self._b))
+        if st != 0:
+            raise KifmmError(st, "kifmm_batch_create failed")
+
+    def eval(self, d_srcden, d_trgval, nrhs: int = 1, stream: int = 0, sync: bool = True) -> int:
+        n = len(self.fmms)
+        src = (ctypes.c_void_p * n)(*d_srcden)
+        dst = (ctypes.c_void_p * n)(*d_trgval)
+        st = lib().kifmm_batch_eval_device(self._b, nrhs, src, dst, ctypes.c_void_p(stream), 1 if sync else 0)
+        if st != 0:
+            raise KifmmError(st, lib().kifmm_batch_last_error(self._b).decode())
+        return 0
+
+    def __del__(self):
+        b = getattr(self, "_b", None)
+        if b is not None and b.value and _lib is not None:
+            _lib.kifmm_batch_destroy(b)
+            self._b = None
 
 
 def header_symbols(header_path: str | None = None):

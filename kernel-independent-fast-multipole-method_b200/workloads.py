@@ -141,3 +141,29 @@ def surface_counts(np_: int):
 def log_uniform_sizes(k: int, lo: float = 1e4, hi: float = 5e5, seed: int = 3):
     u = np.random.default_rng(seed).uniform(math.log(lo), math.log(hi), k)
     return np.round(np.exp(u)).astype(np.int64)
+
+
+def plummer_ball(n: int, seed: int = 0, scale: float = 0.1):
+    """A Plummer-clustered ball of scale radius `scale` at the origin (points
+    outside the open root box (-1,1)^3 redrawn)."""
+    return cube_plummer(n, seed, frac=1.0, scale=scale, centre=(0.0, 0.0, 0.0))
+
+
+GEOMETRIES = {"sphere": sphere, "ellipsoid": ellipsoid, "cube": cube, "cube_plummer": cube_plummer,
+              "plummer_ball": plummer_ball}
+
+
+def batched_instances(k: int = 64, n_stokes: int = 16, seed: int = 3, lo: float = 1e4, hi: float = 5e5):
+    """The batched workload: k independent instances with log-uniform sizes in
+    [lo, hi]; geometries cycle through the unit sphere surface, the uniform
+    cube and the Plummer ball; n_stokes of them (seeded choice) use the Stokes
+    single-layer kernel (311, mu = 1), the rest Laplace single-layer (111)."""
+    sizes = log_uniform_sizes(k, lo, hi, seed)
+    stokes = set(np.random.default_rng(seed + 1).choice(k, size=n_stokes, replace=False).tolist())
+    geoms = ("sphere", "cube", "plummer_ball")
+    out = []
+    for i in range(k):
+        kt = 311 if i in stokes else 111
+        out.append({"index": i, "kt": kt, "coefs": (1.0,), "n": int(sizes[i]), "geometry": geoms[i % 3],
+                    "seed": 100 + i})
+    return out

@@ -1,0 +1,70 @@
+"""Batched evaluation (kifmm_batch_*): several set-up instances, of different
+kernels and precisions, evaluated in one captured CUDA graph.
+
+The graph replays exactly the passes a single eval_device enqueues, so each
+instance's output must be bit-identical to its own eval_device call; a new
+set of buffers or rhs count recaptures the graph.
+"""
+import numpy as np
+import pytest
+
+import golden_cases as G
+import kifmm
+import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def _engine(d, precision):
+    f = kifmm.FMM3d("fmm3d_")
+    f.srcpos, f.srcnor, f.trgpos = d["src"], d["nor"], d["trg"]
+    f.ctr, f.rootlvl = tuple(d["ctr"]), d["rootlvl"]
+    f.knl = kifmm.Kernel3d(d["kt"], d["coefs"])
+    f.setup(G.options(d, precision))
+    return f
+
+
+def test_batch_matches_single_instance_evals(gpu):
+    torch = pytest.importorskip("torch")
+    cases = [("lap_s_np6_tt_style", "mixed"), ("stk_s_np6_cube", "mixed"), ("lap_s_np4_sphere", "fp64"),
+             ("nav_s_np6_sphere", "fp64")]
+    nrhs = 2
+    fmms, srcs, outs, want = [], [], [], []
+    rng = np.random.default_rng(11)
+    for name, prec in cases:
+        d = G.load(name)
+        f = _engine(d, prec)
+        sd, td = W.KERNEL_DOFS[d["kt"]]
+        den = rng.standard_normal(nrhs * sd * len(d["src"]))
+        s = torch.tensor(den, device="cuda", dtype=torch.float64)
+        o = torch.zeros(nrhs * td * len(d["trg"]), device="cuda", dtype=torch.float64)
+        ref = torch.zeros_like(o)
+        f.eval_device(s.data_ptr(), ref.data_ptr(), nrhs, 0, sync=True)
+        fmms.append(f)
+        srcs.append(s)
+        outs.append(o)
+        want.append(ref.cpu().numpy())
+    b = kifmm.Batch(fmms)
+    for _ in range(2):  # capture, then replay
+        for o in outs:
+            o.zero_()
+        torch.cuda.synchronize()
+        b.eval([s.data_ptr() for s in srcs], [o.data_ptr() for o in outs], nrhs, 0, sync=True)
+        for o, w in zip(outs, want):
+            assert np.array_equal(o.cpu().numpy(), w)
+    # other buffers and a single rhs: recaptured
+    outs1 = [torch.zeros(o.numel() // nrhs, device="cuda", dtype=torch.float64) for o in outs]
+    b.eval([s.data_ptr() for s in srcs], [o.data_ptr() for o in outs1], 1, 0, sync=True)
+    for o, w in zip(outs1, want):
+        assert np.array_equal(o.cpu().numpy(), w[: o.numel()])
+
+
+def test_batch_rejects_bad_arguments(gpu):
+    d = G.load("lap_s_np4_sphere")
+    f = _engine(d, "fp64")
+    b = kifmm.Batch([f])
+    with pytest.raises(kifmm.KifmmError):
+        b.eval([0], [0], 0)
+    unset = kifmm.FMM3d("fmm3d_")
+    with pytest.raises(kifmm.KifmmError):
+        kifmm.Batch([unset])
