@@ -95,6 +95,9 @@ struct Impl : ImplBase {
   T *ybuf, *zbuf;  // per-node rank-space coordinates of the upward / downward densities
   int ru = 0, rd = 0;
   T* khat;
+  T* ktiles = nullptr;  // [ceil(nf/32)][343][32] operator spectra for the parent-pair sweep
+  int* h_status = nullptr;  // mapped host word: device-side wait time-outs (bit 0)
+  int* d_status = nullptr;
   List s2m, s2l, leaf, m2l, fwd;
   std::vector<List> up_non, dn_par;
   List up_all, dn_all;
@@ -108,6 +111,7 @@ struct Impl : ImplBase {
   Impl(Engine& e) : E(e), tr(e.tree), op(*e.ops) {}
   ~Impl() override {
     for (void* p : allocs) cudaFree(p);
+    if (h_status) cudaFreeHost(h_status);
     if (have_events)
       for (auto& x : ev) cudaEventDestroy(x);
   }
@@ -188,7 +192,22 @@ struct Impl : ImplBase {
         kh[2 * i + 1] = (T)op.m2l[i].imag();
       }
       khat = upload(kh);
+      if (sd_m == 1 && td_m == 1 && m2l_sweep_supported(op.nfreq)) {
+        const int nf = op.nfreq, ftiles = (nf + 31) / 32;
+        std::vector<T> kt((size_t)ftiles * 343 * 32 * 2, T(0));
+        for (int ft = 0; ft < ftiles; ft++)
+          for (int o = 0; o < 343; o++)
+            for (int l = 0; l < 32 && ft * 32 + l < nf; l++) {
+              size_t dst = (((size_t)ft * 343 + o) * 32 + l) * 2;
+              kt[dst] = kh[((size_t)o * nf + ft * 32 + l) * 2];
+              kt[dst + 1] = kh[((size_t)o * nf + ft * 32 + l) * 2 + 1];
+            }
+        ktiles = upload(kt);
+      }
     }
+    KCHECK(cudaHostAlloc((void**)&h_status, sizeof(int), cudaHostAllocMapped));
+    *h_status = 0;
+    KCHECK(cudaHostGetDevicePointer((void**)&d_status, h_status, 0));
     double kc[3];
     kernel_constants(E.user.kt, E.user.coefs, kc);
     args.ku = KConst<T>{(T)kc[0], (T)kc[1], (T)kc[2]};
@@ -284,11 +303,12 @@ struct Impl : ImplBase {
       m2l = make_list(work, {}, ptr, idx);
       fwd = make_list(fwdn, {});
       effval = dalloc<T>((size_t)nn * td_m * op.nfreq * 2);
-      spectra = dalloc<T>((size_t)nn * sd_m * op.nfreq * 2);
-      // nodes outside every V list keep a zero spectrum (read by the parent-pair form)
-      KCHECK(cudaMemset(spectra, 0, sizeof(T) * (size_t)nn * sd_m * op.nfreq * 2));
+      // nn + 8 blocks: nodes outside every V list keep a zero spectrum, and the
+      // 8 blocks from index nn on stand for an absent colleague (parent-pair form)
+      spectra = dalloc<T>((size_t)(nn + 8) * sd_m * op.nfreq * 2);
+      KCHECK(cudaMemset(spectra, 0, sizeof(T) * (size_t)(nn + 8) * sd_m * op.nfreq * 2));
       counters_v = (double)idx.size();
-      if (sd_m == 1 && td_m == 1) build_pairs(work);
+      if (ktiles) build_pairs(work);
       counters_fwd = (double)fwdn.size();
       counters_inv = (double)work.size();
     }
@@ -383,7 +403,7 @@ struct Impl : ImplBase {
       }
     }
     std::sort(qlist.begin(), qlist.end());
-    std::vector<int> qchd, coll(qlist.size() * 26, -1);
+    std::vector<int> qchd, coll(qlist.size() * 26, tr.nnodes);  // absent: the zero block
     std::vector<unsigned char> mask(qlist.size(), 0);
     for (size_t w = 0; w < qlist.size(); w++) {
       int q = qlist[w];
@@ -488,8 +508,8 @@ struct Impl : ImplBase {
         launch_m2l_forward<T>(geom, supeden, fwd.work, fwd.n, d_depth, spectra, st);
         if (prof && r == 0) KCHECK(cudaEventRecord(ev[7], st));
         if (pairs_n > 0)
-          launch_m2l_hadamard_sweep<T>(op.nfreq, khat, spectra, pairs_n, pairs_chd, pairs_coll, pairs_mask, effval,
-                                       num_sms, st);
+          launch_m2l_hadamard_sweep<T>(op.nfreq, ktiles, spectra, pairs_n, pairs_chd, pairs_coll, pairs_mask, effval,
+                                       tr.nnodes, d_status, num_sms, st);
         else
           launch_m2l_hadamard<T>(geom, khat, spectra, m2l.work, m2l.n, m2l.ptr, m2l.idx, d_path, effval, st);
         if (prof && r == 0) KCHECK(cudaEventRecord(ev[8], st));
@@ -543,6 +563,12 @@ struct Impl : ImplBase {
   }
 
   void reserve(int nrhs) override { ensure_rhs(nrhs); }
+  int take_status() override {
+    volatile int* p = h_status;
+    int v = *p;
+    *p = 0;
+    return v;
+  }
 
   void phase_times(double* ms) const override {
     for (int i = 0; i < 9; i++) ms[i] = pt[i];
@@ -691,7 +717,13 @@ int Engine::eval_device(const double* d_srcden, double* d_trgval, int nrhs, cuda
   try {
     int rc = impl->eval(d_srcden, d_trgval, nrhs, st);  // st as given: NULL is the legacy default stream
     if (rc != KIFMM_OK) return rc;
-    if (sync) KCHECK(cudaStreamSynchronize(st));
+    if (sync) {
+      KCHECK(cudaStreamSynchronize(st));
+      if (impl->take_status()) {
+        err = "a device-side wait timed out; results are incomplete";
+        return KIFMM_ERR_CUDA;
+      }
+    }
   } catch (const CudaError& e) {
     err = std::string(e.where) + ": " + cudaGetErrorString(e.e);
     cudaGetLastError();
@@ -764,6 +796,10 @@ int Engine::eval_host(const double* srcden, double* trgval, int nrhs) {
     if (rc != KIFMM_OK) return rc;
     KCHECK(cudaMemcpyAsync(trgval, d_out, nout * sizeof(double), cudaMemcpyDeviceToHost, stream));
     KCHECK(cudaStreamSynchronize(stream));
+    if (impl->take_status()) {
+      err = "a device-side wait timed out; results are incomplete";
+      return KIFMM_ERR_CUDA;
+    }
   } catch (const CudaError& e) {
     err = std::string(e.where) + ": " + cudaGetErrorString(e.e);
     cudaGetLastError();

@@ -19,6 +19,8 @@ struct ImplBase {
   virtual int eval(const double* d_srcden, double* d_trgval, int nrhs, cudaStream_t st) = 0;
   // grows the per-rhs buffers (no allocation may happen inside a stream capture)
   virtual void reserve(int nrhs) = 0;
+  // reads and clears the device-side error word (bit 0: a bounded wait timed out)
+  virtual int take_status() = 0;
   virtual void phase_times(double* ms) const = 0;
   virtual int launches() const = 0;
 };

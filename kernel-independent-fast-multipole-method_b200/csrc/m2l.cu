@@ -58,12 +58,15 @@ __host__ __device__ inline size_t inv_warp_bytes(int np, int n, int nh) {
          align16(sizeof(Cpx<T>) * np * np * nh);
 }
 
-template <typename T>
+template <typename T, int NP>
 __global__ void __launch_bounds__(256) k_m2l_fwd_warp(M2LGeom g, const T* __restrict__ supeden,
                                                       const int* __restrict__ nodes, int nwork,
                                                       const int* __restrict__ depth, T* __restrict__ spectra) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int np = g.np, n = g.n, nh = g.nh, nf = g.nfreq;
+  // NP > 0: compile-time sizes (constant divisors, unrolled sums); NP = 0: any np
+  const int np = NP > 0 ? NP : g.np, n = NP > 0 ? 2 * NP : g.n, nh = NP > 0 ? NP + 1 : g.nh;
+  const int nf = NP > 0 ? 4 * NP * NP * (NP + 1) : g.nfreq;
+  const int nsurf = NP > 0 ? NP * NP * NP - (NP - 2) * (NP - 2) * (NP - 2) : g.nsurf;
   Cpx<T>* W2 = reinterpret_cast<Cpx<T>*>(smem_raw);
   fill_w2(W2, n);
   __syncthreads();
@@ -75,12 +78,12 @@ __global__ void __launch_bounds__(256) k_m2l_fwd_warp(M2LGeom g, const T* __rest
   for (int wi = blockIdx.x * wpc + warp; wi < nwork; wi += gridDim.x * wpc) {
     const int node = nodes[wi];
     const int lvl = depth[node] + g.rootlvl;
-    const T* den = supeden + (size_t)node * g.nsurf * g.sd;
+    const T* den = supeden + (size_t)node * nsurf * g.sd;
     for (int s = 0; s < g.sd; s++) {
       const T scale = (T)ldexp(1.0, lvl * g.deg[s]);  // plnden2effden scaling, matmgnt3d.cpp:228-235
       for (int e = lane; e < np * np * np; e += 32) xg[e] = T(0);
       __syncwarp();
-      for (int k = lane; k < g.nsurf; k += 32) {
+      for (int k = lane; k < nsurf; k += 32) {
         int i = g.surf_ijk[3 * k], j = g.surf_ijk[3 * k + 1], kk = g.surf_ijk[3 * k + 2];
         xg[(i * np + j) * np + kk] = den[(size_t)k * g.sd + s] * scale;
       }
@@ -88,6 +91,7 @@ __global__ void __launch_bounds__(256) k_m2l_fwd_warp(M2LGeom g, const T* __rest
       for (int e = lane; e < np * np * nh; e += 32) {  // x pass
         int kx = e % nh, j = (e / nh) % np, k = e / (nh * np);
         T re = 0, im = 0;
+#pragma unroll
         for (int i = 0; i < np; i++) {
           T v = xg[(i * np + j) * np + k];
           Cpx<T> t = W2[i * n + kx];
@@ -101,6 +105,7 @@ __global__ void __launch_bounds__(256) k_m2l_fwd_warp(M2LGeom g, const T* __rest
       for (int e = lane; e < np * n * nh; e += 32) {  // y pass
         int kx = e % nh, ky = (e / nh) % n, k = e / (nh * n);
         T re = 0, im = 0;
+#pragma unroll
         for (int j = 0; j < np; j++) {
           Cpx<T> a = A[(k * np + j) * nh + kx];
           Cpx<T> t = W2[j * n + ky];
@@ -116,6 +121,7 @@ __global__ void __launch_bounds__(256) k_m2l_fwd_warp(M2LGeom g, const T* __rest
         int kxy = e % (n * nh), kz = e / (n * nh);
         Cpx<T> r;
         r.re = r.im = T(0);
+#pragma unroll
         for (int k = 0; k < np; k++) {
           Cpx<T> b = Bm[k * n * nh + kxy];
           Cpx<T> t = W2[k * n + kz];
@@ -129,12 +135,15 @@ __global__ void __launch_bounds__(256) k_m2l_fwd_warp(M2LGeom g, const T* __rest
   }
 }
 
-template <typename T>
+template <typename T, int NP>
 __global__ void __launch_bounds__(256) k_m2l_inv_warp(M2LGeom g, const T* __restrict__ effval,
                                                       const int* __restrict__ work, int nwork,
                                                       T* __restrict__ tdncval) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int np = g.np, n = g.n, nh = g.nh, nf = g.nfreq;
+  // NP > 0: compile-time sizes (constant divisors, unrolled sums); NP = 0: any np
+  const int np = NP > 0 ? NP : g.np, n = NP > 0 ? 2 * NP : g.n, nh = NP > 0 ? NP + 1 : g.nh;
+  const int nf = NP > 0 ? 4 * NP * NP * (NP + 1) : g.nfreq;
+  const int nsurf = NP > 0 ? NP * NP * NP - (NP - 2) * (NP - 2) * (NP - 2) : g.nsurf;
   Cpx<T>* W2 = reinterpret_cast<Cpx<T>*>(smem_raw);
   fill_w2(W2, n);
   __syncthreads();
@@ -145,7 +154,7 @@ __global__ void __launch_bounds__(256) k_m2l_inv_warp(M2LGeom g, const T* __rest
   Cpx<T>* A = reinterpret_cast<Cpx<T>*>(reinterpret_cast<unsigned char*>(Bm) + align16(sizeof(Cpx<T>) * np * n * nh));
   for (int wi = blockIdx.x * wpc + warp; wi < nwork; wi += gridDim.x * wpc) {
     const int node = work[wi];
-    T* dst = tdncval + (size_t)node * g.nsurf * g.td;
+    T* dst = tdncval + (size_t)node * nsurf * g.td;
     for (int t = 0; t < g.td; t++) {
       const Cpx<T>* src = reinterpret_cast<const Cpx<T>*>(effval + ((size_t)node * g.td + t) * nf * 2);
       for (int e = lane; e < nf; e += 32) Y[e] = src[e];
@@ -153,6 +162,7 @@ __global__ void __launch_bounds__(256) k_m2l_inv_warp(M2LGeom g, const T* __rest
       for (int e = lane; e < np * n * nh; e += 32) {  // z pass (inverse), k < np
         int kxy = e % (n * nh), k = e / (n * nh);
         T re = 0, im = 0;
+#pragma unroll
         for (int kz = 0; kz < n; kz++) {
           Cpx<T> y = Y[kz * n * nh + kxy];
           Cpx<T> c = W2[k * n + kz];
@@ -166,6 +176,7 @@ __global__ void __launch_bounds__(256) k_m2l_inv_warp(M2LGeom g, const T* __rest
       for (int e = lane; e < np * np * nh; e += 32) {  // y pass (inverse), j < np
         int kx = e % nh, j = (e / nh) % np, k = e / (nh * np);
         T re = 0, im = 0;
+#pragma unroll
         for (int ky = 0; ky < n; ky++) {
           Cpx<T> b = Bm[(k * n + ky) * nh + kx];
           Cpx<T> c = W2[j * n + ky];
@@ -176,11 +187,12 @@ __global__ void __launch_bounds__(256) k_m2l_inv_warp(M2LGeom g, const T* __rest
         A[e].im = im;
       }
       __syncwarp();
-      for (int m = lane; m < g.nsurf; m += 32) {  // c2r along x at the surface points
+      for (int m = lane; m < nsurf; m += 32) {  // c2r along x at the surface points
         int i = g.surf_ijk[3 * m], j = g.surf_ijk[3 * m + 1], k = g.surf_ijk[3 * m + 2];
         const Cpx<T>* a = &A[(k * np + j) * nh];
         T v = a[0].re + ((i & 1) ? -a[nh - 1].re : a[nh - 1].re);
         T acc = 0;
+#pragma unroll
         for (int kx = 1; kx < nh - 1; kx++) {
           Cpx<T> c = W2[i * n + kx];
           acc += a[kx].re * c.re + a[kx].im * c.im;
@@ -260,9 +272,13 @@ void launch_m2l_forward(const M2LGeom& g, const T* supeden, const int* nodes, in
   const size_t head = align16(sizeof(Cpx<T>) * g.n * g.n);
   int wpc = (int)std::max<size_t>(1, std::min<size_t>(8, (200 * 1024 - head) / per_warp));
   size_t smem = head + per_warp * wpc;
-  cudaFuncSetAttribute(k_m2l_fwd_warp<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int grid = std::max(1, std::min((nn + wpc - 1) / wpc, 148 * 8));
-  k_m2l_fwd_warp<T><<<grid, 32 * wpc, smem, st>>>(g, supeden, nodes, nn, depth, spectra);
+  auto kern = g.np == 6 ? k_m2l_fwd_warp<T, 6>
+              : g.np == 4 ? k_m2l_fwd_warp<T, 4>
+              : g.np == 8 ? k_m2l_fwd_warp<T, 8>
+                          : k_m2l_fwd_warp<T, 0>;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  kern<<<grid, 32 * wpc, smem, st>>>(g, supeden, nodes, nn, depth, spectra);
 }
 
 template <typename T>
@@ -284,9 +300,13 @@ void launch_m2l_inverse(const M2LGeom& g, const T* effval, const int* work, int 
   const size_t head = align16(sizeof(Cpx<T>) * g.n * g.n);
   int wpc = (int)std::max<size_t>(1, std::min<size_t>(8, (200 * 1024 - head) / per_warp));
   size_t smem = head + per_warp * wpc;
-  cudaFuncSetAttribute(k_m2l_inv_warp<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int grid = std::max(1, std::min((nwork + wpc - 1) / wpc, 148 * 8));
-  k_m2l_inv_warp<T><<<grid, 32 * wpc, smem, st>>>(g, effval, work, nwork, tdncval);
+  auto kern = g.np == 6 ? k_m2l_inv_warp<T, 6>
+              : g.np == 4 ? k_m2l_inv_warp<T, 4>
+              : g.np == 8 ? k_m2l_inv_warp<T, 8>
+                          : k_m2l_inv_warp<T, 0>;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  kern<<<grid, 32 * wpc, smem, st>>>(g, effval, work, nwork, tdncval);
 }
 
 // ---------------------------------------------------------------------------
@@ -305,37 +325,92 @@ void launch_m2l_inverse(const M2LGeom& g, const T* effval, const int* work, int 
 // time and its source spectra (nodes x 32 freq x 8 B, ~93 MB at 4M points)
 // stay in L2 for their 26-fold reuse.  The next colleague's 8 child spectra
 // are loaded into registers while the current colleague is multiplied.
-template <typename T, int QPT, int NTHR>
-__global__ void __launch_bounds__(NTHR) k_m2l_had_sweep(int nf, const T* __restrict__ khat,
-                                                       const T* __restrict__ spectra, int nq,
+//
+// The operator tile of a frequency tile (all 343 offsets x 32 frequencies,
+// zero for |o| <= 1, stored contiguously per tile) is staged into shared
+// memory by one bulk asynchronous copy completing on an mbarrier; with two
+// buffers (FP32) the next tile's copy runs under the current tile's work.
+// NF (frequencies per node) is a template argument, so the 8 child spectra
+// of a colleague are 8 loads at immediate offsets from one address.  Absent
+// colleagues point at an all-zero spectrum block (zero_node), so the loads
+// need no predicate.  Every mbarrier wait is bounded: on time-out the kernel
+// sets bit 0 of *status and returns.
+namespace {
+
+__device__ __constant__ short c_dir_base[26] = {57,  59,  61,  71,  73,  75,  85,  87,  89,  155, 157, 159, 169,
+                                               173, 183, 185, 187, 253, 255, 257, 267, 269, 271, 281, 283, 285};
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void bulk_load(unsigned dst, const void* src, unsigned bytes, unsigned bar) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned parity) {
+  for (int it = 0; it < (1 << 22); it++) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
+template <typename T, int NF, int QPT, int NTHR, int NBUF>
+__global__ void __launch_bounds__(NTHR) k_m2l_had_sweep(const Cpx<T>* __restrict__ ktiles,
+                                                       const Cpx<T>* __restrict__ spectra, int nq,
                                                        const int* __restrict__ qchd, const int* __restrict__ coll,
                                                        const unsigned char* __restrict__ mask,
-                                                       T* __restrict__ effval) {
+                                                       Cpx<T>* __restrict__ effval, int zero_node,
+                                                       int* __restrict__ status) {
+  constexpr int TILE = 343 * 32;
+  constexpr unsigned TILE_BYTES = TILE * sizeof(Cpx<T>);
+  constexpr int FTILES = (NF + 31) / 32;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  Cpx<T>* Ks = reinterpret_cast<Cpx<T>*>(smem_raw);  // [343][32]: every offset in [-3,3]^3, zero when |o| <= 1
+  Cpx<T>* Kbuf = reinterpret_cast<Cpx<T>*>(smem_raw);  // NBUF x [343][32]
+  __shared__ __align__(8) unsigned long long bars[NBUF];
   __shared__ int next_q;  // next unclaimed group of the CTA's slice, per frequency tile
   const int lane = threadIdx.x & 31;
   const int per_cta = (nq + gridDim.x - 1) / gridDim.x;
   const int qbeg = blockIdx.x * per_cta;
   const int qend = min(nq, qbeg + per_cta);
-  const int ftiles = (nf + 31) / 32;
-  for (int ft = 0; ft < ftiles; ft++) {
-    const int f0 = ft * 32;
-    const int f = f0 + lane;
-    const bool fv = f < nf;
-    __syncthreads();
-    if (threadIdx.x == 0) next_q = qbeg;
-    for (int e = threadIdx.x; e < 343 * 32; e += blockDim.x) {
-      int o = e >> 5, l = e & 31;
-      Cpx<T> v;
-      v.re = v.im = T(0);
-      if (f0 + l < nf) {
-        v.re = khat[((size_t)o * nf + f0 + l) * 2];
-        v.im = khat[((size_t)o * nf + f0 + l) * 2 + 1];
-      }
-      Ks[e] = v;
+  if (threadIdx.x == 0) {
+    for (int b = 0; b < NBUF; b++) mbar_init(smem_addr(&bars[b]), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    if (NBUF == 2) bulk_load(smem_addr(Kbuf), ktiles, TILE_BYTES, smem_addr(&bars[0]));
+  }
+  __syncthreads();
+  for (int ft = 0; ft < FTILES; ft++) {
+    const int buf = NBUF == 2 ? (ft & 1) : 0;
+    const unsigned parity = NBUF == 2 ? ((ft >> 1) & 1) : (ft & 1);
+    if (threadIdx.x == 0) {
+      next_q = qbeg;
+      // the buffer written here was last read in tile ft-1, which every warp
+      // has finished (barrier at the end of the previous iteration)
+      if (NBUF == 2 && ft + 1 < FTILES)
+        bulk_load(smem_addr(Kbuf + (size_t)((ft + 1) & 1) * TILE), ktiles + (size_t)(ft + 1) * TILE, TILE_BYTES,
+                  smem_addr(&bars[(ft + 1) & 1]));
+      if (NBUF == 1) bulk_load(smem_addr(Kbuf), ktiles + (size_t)ft * TILE, TILE_BYTES, smem_addr(&bars[0]));
     }
     __syncthreads();
+    const bool ok = mbar_wait_bounded(smem_addr(&bars[buf]), parity);
+    if (__syncthreads_or(!ok)) {
+      if (threadIdx.x == 0) atomicOr(status, 1);
+      return;
+    }
+    const Cpx<T>* Ks = Kbuf + (size_t)buf * TILE;
+    const int f = ft * 32 + lane;
+    const int fl = min(f, NF - 1);  // lanes past NF load a valid spectrum and store nothing
     // warps claim QPT target parents at a time, so they finish the tile together
     while (true) {
       int q0 = 0;
@@ -347,28 +422,28 @@ __global__ void __launch_bounds__(NTHR) k_m2l_had_sweep(int nf, const T* __restr
       for (int q = 0; q < QPT; q++)
 #pragma unroll
         for (int i = 0; i < 8; i++) ar[q][i] = ai[q][i] = T(0);
-      // prefetch colleague 0
+      const int* cq[QPT];
+#pragma unroll
+      for (int q = 0; q < QPT; q++) cq[q] = coll + (size_t)min(q0 + q, qend - 1) * 26;
       int nb[QPT];
       T nxr[QPT][8], nxi[QPT][8];
 #pragma unroll
-      for (int q = 0; q < QPT; q++) nb[q] = (q0 + q < qend) ? coll[(size_t)(q0 + q) * 26] : -1;
-#pragma unroll
-      for (int q = 0; q < QPT; q++)
+      for (int q = 0; q < QPT; q++) {
+        nb[q] = (q0 + q < qend) ? cq[q][0] : zero_node;
+        const Cpx<T>* X = spectra + (size_t)nb[q] * NF + fl;
 #pragma unroll
         for (int j = 0; j < 8; j++) {
-          nxr[q][j] = nxi[q][j] = T(0);
-          if (nb[q] >= 0 && fv) {
-            const T* X = spectra + ((size_t)(nb[q] + j) * nf + f) * 2;
-            nxr[q][j] = X[0];
-            nxi[q][j] = X[1];
-          }
+          Cpx<T> x = X[j * NF];
+          nxr[q][j] = x.re;
+          nxi[q][j] = x.im;
         }
+      }
       for (int dir = 0; dir < 26; dir++) {
         T xr[QPT][8], xi[QPT][8];
         bool any = false;
 #pragma unroll
         for (int q = 0; q < QPT; q++) {
-          any |= nb[q] >= 0;
+          any |= nb[q] != zero_node;
 #pragma unroll
           for (int j = 0; j < 8; j++) {
             xr[q][j] = nxr[q][j];
@@ -377,32 +452,28 @@ __global__ void __launch_bounds__(NTHR) k_m2l_had_sweep(int nf, const T* __restr
         }
         if (dir + 1 < 26) {
 #pragma unroll
-          for (int q = 0; q < QPT; q++) nb[q] = (q0 + q < qend) ? coll[(size_t)(q0 + q) * 26 + dir + 1] : -1;
-#pragma unroll
-          for (int q = 0; q < QPT; q++)
+          for (int q = 0; q < QPT; q++) {
+            nb[q] = (q0 + q < qend) ? cq[q][dir + 1] : zero_node;
+            const Cpx<T>* X = spectra + (size_t)nb[q] * NF + fl;
 #pragma unroll
             for (int j = 0; j < 8; j++) {
-              nxr[q][j] = nxi[q][j] = T(0);
-              if (nb[q] >= 0 && fv) {
-                const T* X = spectra + ((size_t)(nb[q] + j) * nf + f) * 2;
-                nxr[q][j] = X[0];
-                nxi[q][j] = X[1];
-              }
+              Cpx<T> x = X[j * NF];
+              nxr[q][j] = x.re;
+              nxi[q][j] = x.im;
             }
+          }
         }
         if (!any) continue;
         // offset of child j of P from child i of Q: 2*dir + oct(j) - oct(i); the
         // adjacent pairs (|offset| <= 1) read the zero rows of the tile
-        const int dd = dir < 13 ? dir : dir + 1;
-        const int base = (2 * (dd / 9 - 1) + 3) * 49 + (2 * ((dd / 3) % 3 - 1) + 3) * 7 + (2 * (dd % 3 - 1) + 3);
-        const Cpx<T>* Kd = Ks + base * 32 + lane;
+        const Cpx<T>* Kd = Ks + c_dir_base[dir] * 32 + lane;
 #pragma unroll
         for (int j = 0; j < 8; j++) {
 #pragma unroll
           for (int i = 0; i < 8; i++) {
             const int cij = (((j >> 2) & 1) - ((i >> 2) & 1)) * 49 + (((j >> 1) & 1) - ((i >> 1) & 1)) * 7 +
                             ((j & 1) - (i & 1));
-            Cpx<T> k = Kd[cij * 32];
+            const Cpx<T> k = Kd[cij * 32];
 #pragma unroll
             for (int q = 0; q < QPT; q++) {
               ar[q][i] += k.re * xr[q][j] - k.im * xi[q][j];
@@ -411,41 +482,63 @@ __global__ void __launch_bounds__(NTHR) k_m2l_had_sweep(int nf, const T* __restr
           }
         }
       }
-      if (fv) {
+      if (f < NF) {
 #pragma unroll
         for (int q = 0; q < QPT; q++) {
           if (q0 + q >= qend) continue;
-          int c0 = qchd[q0 + q];
-          unsigned m = mask[q0 + q];
+          const int c0 = qchd[q0 + q];
+          const unsigned m = mask[q0 + q];
 #pragma unroll
           for (int i = 0; i < 8; i++) {
             if (!((m >> i) & 1)) continue;
-            T* Y = effval + ((size_t)(c0 + i) * nf + f) * 2;
-            Y[0] = ar[q][i];
-            Y[1] = ai[q][i];
+            Cpx<T> y;
+            y.re = ar[q][i];
+            y.im = ai[q][i];
+            effval[(size_t)(c0 + i) * NF + f] = y;
           }
         }
       }
     }
+    __syncthreads();
   }
 }
 
-template <typename T>
-void launch_m2l_hadamard_sweep(int nf, const T* khat, const T* spectra, int nq, const int* qchd, const int* coll,
-                               const unsigned char* mask, T* effval, int num_sms, cudaStream_t st) {
-  if (nq <= 0) return;
+template <typename T, int NF>
+void sweep_launch(const T* ktiles, const T* spectra, int nq, const int* qchd, const int* coll,
+                  const unsigned char* mask, T* effval, int zero_node, int* status, int num_sms, cudaStream_t st) {
   constexpr int QPT = 2;
-  size_t smem = sizeof(Cpx<T>) * 343 * 32;
-  // one CTA per SM: 16 warps (FP32) or 8 warps (FP64, twice the registers) share one operator tile
+  // one CTA per SM: 16 warps (FP32, operator tile double-buffered) or 8 warps
+  // (FP64: twice the registers, one 176 KB tile)
   constexpr int NTHR = sizeof(T) == 4 ? 512 : 256;
-  cudaFuncSetAttribute(k_m2l_had_sweep<T, QPT, NTHR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  constexpr int NBUF = sizeof(T) == 4 ? 2 : 1;
+  const size_t smem = (size_t)NBUF * 343 * 32 * sizeof(Cpx<T>);
+  auto kern = k_m2l_had_sweep<T, NF, QPT, NTHR, NBUF>;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int grid = std::max(1, std::min(num_sms, (nq + QPT - 1) / QPT));
-  k_m2l_had_sweep<T, QPT, NTHR><<<grid, NTHR, smem, st>>>(nf, khat, spectra, nq, qchd, coll, mask, effval);
+  kern<<<grid, NTHR, smem, st>>>(reinterpret_cast<const Cpx<T>*>(ktiles), reinterpret_cast<const Cpx<T>*>(spectra),
+                                 nq, qchd, coll, mask, reinterpret_cast<Cpx<T>*>(effval), zero_node, status);
+}
+
+}  // namespace
+
+bool m2l_sweep_supported(int nf) { return nf == 320 || nf == 1008 || nf == 2304; }
+
+template <typename T>
+void launch_m2l_hadamard_sweep(int nf, const T* ktiles, const T* spectra, int nq, const int* qchd, const int* coll,
+                               const unsigned char* mask, T* effval, int zero_node, int* status, int num_sms,
+                               cudaStream_t st) {
+  if (nq <= 0) return;
+  if (nf == 1008)
+    sweep_launch<T, 1008>(ktiles, spectra, nq, qchd, coll, mask, effval, zero_node, status, num_sms, st);
+  else if (nf == 320)
+    sweep_launch<T, 320>(ktiles, spectra, nq, qchd, coll, mask, effval, zero_node, status, num_sms, st);
+  else if (nf == 2304)
+    sweep_launch<T, 2304>(ktiles, spectra, nq, qchd, coll, mask, effval, zero_node, status, num_sms, st);
 }
 
 #define KIFMM_INST(T)                                                                                             \
   template void launch_m2l_hadamard_sweep<T>(int, const T*, const T*, int, const int*, const int*,               \
-                                             const unsigned char*, T*, int, cudaStream_t);                         \
+                                             const unsigned char*, T*, int, int*, int, cudaStream_t);              \
   template void launch_m2l_forward<T>(const M2LGeom&, const T*, const int*, int, const int*, T*, cudaStream_t);  \
   template void launch_m2l_hadamard<T>(const M2LGeom&, const T*, const T*, const int*, int, const int64_t*,     \
                                        const int*, const int*, T*, cudaStream_t);                                \
