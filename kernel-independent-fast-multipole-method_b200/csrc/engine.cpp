@@ -91,12 +91,20 @@ struct Impl : ImplBase {
   T *sden = nullptr, *tval = nullptr;
   int cap_rhs = 0;
   T *supeden, *supcval, *tdncval, *tdneden, *spectra, *effval;
-  T *A_upW, *A_upV, *A_m2my, *A_dnW, *A_dnV, *A_l2lz;  // factored surface operators
+  // A surface operator: row-major M x K in T (SIMT path) and, for FP32 data,
+  // the split-TF32 pair for the tensor-core path.
+  struct SurfOp {
+    const T* a = nullptr;
+    TcOperator tc;
+    int M = 0, K = 0;
+  };
+  SurfOp op_upW, op_upV, op_m2my, op_dnW, op_dnV, op_l2lz;  // factored surface operators
   T *ybuf, *zbuf;  // per-node rank-space coordinates of the upward / downward densities
-  int ru = 0, rd = 0;
+  int ru = 0, rd = 0;  // ranks rounded up to multiples of 8 (zero-padded rows / columns)
+  bool use_tc = false;
   T* khat;
   T* ktiles = nullptr;  // [ceil(nf/32)][343][32] operator spectra for the parent-pair sweep
-  int* h_status = nullptr;  // mapped host word: device-side wait time-outs (bit 0)
+  int* h_status = nullptr;  // mapped host word: device-side wait time-outs (bit 0 sweep, bit 1 GEMM)
   int* d_status = nullptr;
   List s2m, s2l, leaf, m2l, fwd;
   std::vector<List> up_non, dn_par;
@@ -177,14 +185,7 @@ struct Impl : ImplBase {
     args.uc_unit = upload_as_T(op.uc);
     args.de_unit = upload_as_T(op.de);
     args.dc_unit = upload_as_T(op.dc);
-    ru = op.rank_up;
-    rd = op.rank_dn;
-    A_upW = upload_as_T(op.up_W);
-    A_upV = upload_as_T(op.up_V);
-    A_m2my = upload_as_T(op.m2m_y);
-    A_dnW = upload_as_T(op.dn_W);
-    A_dnV = upload_as_T(op.dn_V);
-    A_l2lz = upload_as_T(op.l2l_z);
+    build_surface_ops();
     {
       std::vector<T> kh(op.m2l.size() * 2);
       for (size_t i = 0; i < op.m2l.size(); i++) {
@@ -383,6 +384,59 @@ struct Impl : ImplBase {
     ensure_rhs(1);
   }
 
+  SurfOp make_op(const std::vector<double>& A, int M, int K) {
+    SurfOp o;
+    o.M = M;
+    o.K = K;
+    o.a = upload_as_T(A);
+    if constexpr (sizeof(T) == 4) {
+      if (use_tc && M % 4 == 0 && K % 4 == 0) {
+        std::vector<float> hi, lo;
+        split_tf32(M, K, A.data(), &hi, &lo, &o.tc.Np, &o.tc.Kp);
+        o.tc.hi = upload(hi);
+        o.tc.lo = upload(lo);
+        o.tc.M = M;
+        o.tc.K = K;
+      }
+    }
+    return o;
+  }
+
+  // The factored operators with both ranks rounded up to multiples of 8, so
+  // that every rank-space vector starts on a 32-byte boundary; the padding
+  // rows and columns are zero, and so are the padded coordinates.
+  void build_surface_ops() {
+    const int r0u = op.rank_up, r0d = op.rank_dn;
+    ru = (r0u + 7) / 8 * 8;
+    rd = (r0d + 7) / 8 * 8;
+    const int K1 = nsurf * sd_m, Kuc = nuc * td_m, Kdc = nsurf * td_m;
+    use_tc = sizeof(T) == 4 && E.tensor_cores && K1 % 4 == 0 && Kuc % 4 == 0 && Kdc % 4 == 0;
+    std::vector<double> upW((size_t)ru * Kuc, 0.0), upV((size_t)K1 * ru, 0.0), m2my((size_t)ru * 8 * ru, 0.0);
+    std::vector<double> dnW((size_t)rd * Kdc, 0.0), dnV((size_t)K1 * rd, 0.0), l2lz((size_t)8 * rd * rd, 0.0);
+    for (int r = 0; r < r0u; r++)
+      for (int k = 0; k < Kuc; k++) upW[(size_t)r * Kuc + k] = op.up_W[(size_t)r * Kuc + k];
+    for (int i = 0; i < K1; i++)
+      for (int r = 0; r < r0u; r++) upV[(size_t)i * ru + r] = op.up_V[(size_t)i * r0u + r];
+    for (int r = 0; r < r0u; r++)
+      for (int o = 0; o < 8; o++)
+        for (int c = 0; c < r0u; c++)
+          m2my[(size_t)r * 8 * ru + (size_t)o * ru + c] = op.m2m_y[(size_t)r * 8 * r0u + (size_t)o * r0u + c];
+    for (int r = 0; r < r0d; r++)
+      for (int k = 0; k < Kdc; k++) dnW[(size_t)r * Kdc + k] = op.dn_W[(size_t)r * Kdc + k];
+    for (int i = 0; i < K1; i++)
+      for (int r = 0; r < r0d; r++) dnV[(size_t)i * rd + r] = op.dn_V[(size_t)i * r0d + r];
+    for (int o = 0; o < 8; o++)
+      for (int r = 0; r < r0d; r++)
+        for (int c = 0; c < r0d; c++)
+          l2lz[((size_t)o * rd + r) * rd + c] = op.l2l_z[((size_t)o * r0d + r) * r0d + c];
+    op_upW = make_op(upW, ru, Kuc);
+    op_upV = make_op(upV, K1, ru);
+    op_m2my = make_op(m2my, ru, 8 * ru);
+    op_dnW = make_op(dnW, rd, Kdc);
+    op_dnV = make_op(dnV, K1, rd);
+    op_l2lz = make_op(l2lz, 8 * rd, rd);
+  }
+
   // Parent-pair form of the V list (single-dof equivalent kernels): one work
   // item per target parent Q with its 26 colleague parents' first-child ids.
   int pairs_n = 0, num_sms = 148;
@@ -459,13 +513,20 @@ struct Impl : ImplBase {
   }
 
   // col_lvl set: output rows scaled by 2^(-(depth + rootlvl) * deg)
-  void gemm(int M, int K, const T* A, const T* B, int64_t ldb, const int* bidx, T* C, int64_t ldc, const int* cidx,
-            int ncol, bool acc, cudaStream_t st, const int* col_lvl = nullptr) {
+  void gemm(const SurfOp& A, const T* B, int64_t ldb, const int* bidx, T* C, int64_t ldc, const int* cidx, int ncol,
+            bool acc, cudaStream_t st, const int* col_lvl = nullptr) {
     if (ncol <= 0) return;
     GemmScale s = scl;
     s.col_lvl = col_lvl;
     s.lvl_base = E.rootlvl;
-    nlaunch += launch_node_gemm<T>(M, K, A, B, ldb, bidx, C, ldc, cidx, ncol, acc, s, gemm_ws, gemm_ws_len, num_sms, st);
+    if constexpr (sizeof(T) == 4) {
+      if (A.tc.hi && ldb % 4 == 0 && ldc % 4 == 0) {
+        nlaunch += launch_node_gemm_tc(A.tc, B, ldb, bidx, C, ldc, cidx, ncol, acc, s, d_status, st);
+        return;
+      }
+    }
+    nlaunch += launch_node_gemm<T>(A.M, A.K, A.a, B, ldb, bidx, C, ldc, cidx, ncol, acc, s, gemm_ws, gemm_ws_len,
+                                   num_sms, st);
   }
 
   void p2p(const List& l, int which, int rhs, cudaStream_t st) {
@@ -495,12 +556,12 @@ struct Impl : ImplBase {
       p2p(s2m, P2P_S2M, r, st);
       // y = up_W * check on the leaves of every level at once, M2M bottom-up
       // in y coordinates, then every node's density = 2^(-l deg) up_V * y
-      gemm(ru, nuc * td_m, A_upW, supcval, (int64_t)nuc * td_m, s2m.work, ybuf, ru, s2m.work, s2m.n, false, st);
+      gemm(op_upW, supcval, (int64_t)nuc * td_m, s2m.work, ybuf, ru, s2m.work, s2m.n, false, st);
       for (int d = md - 1; d >= 2; d--) {
         const List& P = up_non[d];
-        gemm(ru, 8 * ru, A_m2my, ybuf, ru, P.aux, ybuf, ru, P.work, P.n, false, st);
+        gemm(op_m2my, ybuf, ru, P.aux, ybuf, ru, P.work, P.n, false, st);
       }
-      gemm(K1, ru, A_upV, ybuf, ru, up_all.work, supeden, K1, up_all.work, up_all.n, false, st, up_all.aux);
+      gemm(op_upV, ybuf, ru, up_all.work, supeden, K1, up_all.work, up_all.n, false, st, up_all.aux);
       if (prof && r == 0) KCHECK(cudaEventRecord(ev[1], st));
       // V list
       KCHECK(cudaMemsetAsync(tdncval, 0, sizeof(T) * (size_t)tr.nnodes * nsurf * td_m, st));
@@ -524,13 +585,12 @@ struct Impl : ImplBase {
       // z = dn_W * check on the target nodes of every level at once, L2L
       // top-down in z coordinates into the 8 children, then every node's
       // density = 2^(-l deg) dn_V * z
-      gemm(rd, nsurf * td_m, A_dnW, tdncval, (int64_t)nsurf * td_m, dn_all.work, zbuf, rd, dn_all.work, dn_all.n, false,
-           st);
+      gemm(op_dnW, tdncval, (int64_t)nsurf * td_m, dn_all.work, zbuf, rd, dn_all.work, dn_all.n, false, st);
       for (int d = 3; d <= md; d++) {
         const List& P = dn_par[d];
-        gemm(8 * rd, rd, A_l2lz, zbuf, rd, P.work, zbuf, rd, P.aux, P.n, true, st);
+        gemm(op_l2lz, zbuf, rd, P.work, zbuf, rd, P.aux, P.n, true, st);
       }
-      gemm(K1, rd, A_dnV, zbuf, rd, dn_all.work, tdneden, K1, dn_all.work, dn_all.n, false, st, dn_all.aux);
+      gemm(op_dnV, zbuf, rd, dn_all.work, tdneden, K1, dn_all.work, dn_all.n, false, st, dn_all.aux);
       if (prof && r == 0) KCHECK(cudaEventRecord(ev[4], st));
       // leaves
       p2p(leaf, P2P_LEAF, r, st);
@@ -647,6 +707,15 @@ int Engine::setup() {
       err = "precision must be fp64 or mixed";
       return KIFMM_ERR_OPTION;
     }
+  }
+  {
+    bool found = false;
+    int tc = 1;
+    if (!parse_int(opts, "-" + prefix + "tensor_cores", &tc, &found)) {
+      err = "tensor_cores must be 0 or 1";
+      return KIFMM_ERR_OPTION;
+    }
+    tensor_cores = tc != 0;
   }
   if (!equivalent_kernel(user, &mm)) {
     err = "kernel not supported by FMM3d";

@@ -39,6 +39,7 @@ struct Engine {
   // options
   int np = 6, ptsmax = 150, maxlevel = 10;
   bool mixed = false;
+  bool tensor_cores = true;  // mixed mode: surface contractions on tcgen05 (split TF32)
   bool profiling = false;
   // state
   bool ready = false;       // device state built, eval allowed

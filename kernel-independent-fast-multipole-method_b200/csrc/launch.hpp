@@ -3,6 +3,8 @@
 #pragma once
 
 #include <cuda_runtime.h>
+
+#include <vector>
 #include <stdint.h>
 
 #include "kernels_common.cuh"
@@ -53,13 +55,10 @@ template <typename T>
 void launch_gather_val(const T* tval, const int* perm, int nt, int td, int nrhs, double* trgval, cudaStream_t st);
 
 // Batched node GEMM: for j < ncol,
-//   C[cidx[j]*ldc + r] (=|+=) rs(r) * sum_k A[r*K + k] * ks(k) * B[bidx[j]*ldb + k]
-// with rs(r) = 2^(-out_lvl*deg[r % sd]) and ks(k) = 2^(in_lvl*deg[k % sd])
-// when the respective scaling is enabled.  A is M x K row-major.
-// When col_lvl is set, column j uses out level col_lvl[j] + lvl_base instead
-// of out_lvl (one launch then covers nodes of every level).
-// Output row r of column j is multiplied by 2^(-(col_lvl[j] + lvl_base) *
-// deg[r % sd]) when col_lvl is set (homogeneous level scaling).
+//   C[cidx[j]*ldc + r] (=|+=) rs(j, r) * sum_k A[r*K + k] * B[bidx[j]*ldb + k]
+// A is M x K row-major.  rs(j, r) = 2^(-(col_lvl[j] + lvl_base) * deg[r % sd])
+// when col_lvl is set (homogeneous level scaling, one launch covering nodes of
+// every level), else 1.
 struct GemmScale {
   int sd = 1;
   int deg[4] = {0, 0, 0, 0};
@@ -73,6 +72,25 @@ template <typename T>
 int launch_node_gemm(int M, int K, const T* A, const T* B, int64_t ldb, const int* bidx, T* C, int64_t ldc,
                       const int* cidx, int ncol, bool accumulate, const GemmScale& sc, double* ws, size_t ws_len,
                       int num_sms, cudaStream_t st);
+
+// The same product on the tensor cores (tcgen05, kind::tf32) for FP32 data,
+// with both operands split into a TF32 head and a TF32 tail and three MMAs
+// (head*head + head*tail + tail*head) accumulating in FP32 in tensor memory:
+// about 2^-21 relative per product, the FP32 rounding class.  The operator is
+// pre-split on the host: hi/lo are Np x Kp row-major (Np = M rounded up to 16,
+// Kp = K rounded up to 32, zero padded).  Requires K, ldb, ldc multiples of 4
+// and 16-byte aligned B and C.  A bounded wait that times out sets bit 1 of
+// *status.  Returns the number of launches.
+struct TcOperator {
+  const float* hi = nullptr;
+  const float* lo = nullptr;
+  int M = 0, K = 0, Np = 0, Kp = 0;
+};
+int launch_node_gemm_tc(const TcOperator& A, const float* B, int64_t ldb, const int* bidx, float* C, int64_t ldc,
+                        const int* cidx, int ncol, bool accumulate, const GemmScale& sc, int* status,
+                        cudaStream_t st);
+// host-side split of a row-major M x K operator into the padded hi/lo pair
+void split_tf32(int M, int K, const double* A, std::vector<float>* hi, std::vector<float>* lo, int* Np, int* Kp);
 
 // FFT-based M2L (MatMgnt3d::plnden2effden / UE2DC_dgemv / effval2plnval,
 // fmm3d/matmgnt3d.cpp:223-361).

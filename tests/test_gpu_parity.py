@@ -190,3 +190,28 @@ def test_eval_argument_errors(gpu):
         f.eval(d["den"][:-1], np.zeros(len(d["trg"])))
     with pytest.raises(kifmm.KifmmError):
         f.eval(d["den"], np.zeros(len(d["trg"]) + 1))
+
+
+@pytest.mark.parametrize("name", ["lap_s_np6_tt_style", "stk_s_np6_cube", "lap_s_np8_plummer", "nav_s_np6_sphere"])
+def test_mixed_tensor_core_contractions_match_simt(gpu, name):
+    """The tcgen05 split-TF32 surface contractions against the FP32 SIMT
+    ones on the same engine: both are FP32-class, so they agree to 1e-5
+    relative (and each meets the mixed accuracy bound of this file)."""
+    d = G.load(name)
+    td = W.KERNEL_DOFS[d["kt"]][1]
+    outs = []
+    for tc in ("1", "0"):
+        f = kifmm.FMM3d("fmm3d_")
+        f.srcpos, f.srcnor, f.trgpos = d["src"], d["nor"], d["trg"]
+        f.ctr, f.rootlvl = tuple(d["ctr"]), d["rootlvl"]
+        f.knl = kifmm.Kernel3d(d["kt"], d["coefs"])
+        o = G.options(d, "mixed")
+        o["-fmm3d_tensor_cores"] = tc
+        f.setup(o)
+        out = np.zeros(td * len(d["trg"]))
+        f.eval(d["den"], out)
+        outs.append(out)
+        err = oracle.relerr(out.reshape(-1, td)[d["chk"]], d["ref_direct"])
+        assert err <= max(10 * d["ref_relerr"], MIXED_FLOOR), (tc, err, d["ref_relerr"])
+    diff = np.linalg.norm(outs[0] - outs[1]) / np.linalg.norm(outs[1])
+    assert diff <= 1e-5, diff
