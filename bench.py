@@ -15,7 +15,7 @@ point cloud; setup (tree, lists, operators) is done once, outside timing.
              ball), 8 density vectors each, as one captured CUDA graph:
              aggregate point-evaluations/s, mixed and FP64, with per-instance
              errors against the direct sum
-  e2e       Mpoints/s through the host-pointer C API (kifmm_eval): H2D of the
+  e2e        Mpoints/s through the host-pointer C API (kifmm_eval): H2D of the
              densities and D2H of the potentials inside the timed region
   relerr     ||fmm - direct|| / ||fmm|| at 4096 check targets against the
              FP64 direct sum (the reference's FMM3d::check metric)
@@ -411,7 +411,7 @@ def engine_arm(args):
     hbm, peak_kind = peaks()
     # dominant kernel: the M2L Hadamard accumulation; algorithmic bytes per launch =
     # source spectra read once + accumulated target spectra written once + operator spectra
-    nf = 12 * 12 * 7
+    nf = 4 * 6 ** 3 + 4  # independent (Hermitian-canonical) frequencies at np=6
     cplx = 8  # FP32 complex
     alg_bytes = (wc["fwd_spectra"] + wc["inv_spectra"]) * nf * cplx + 316 * nf * cplx
     had_ms = phases.get("m2l_hadamard") or phases["vlist"]

@@ -193,8 +193,8 @@ struct Impl : ImplBase {
         kh[2 * i + 1] = (T)op.m2l[i].imag();
       }
       khat = upload(kh);
-      if (sd_m == 1 && td_m == 1 && m2l_sweep_supported(op.nfreq)) {
-        const int nf = op.nfreq, ftiles = (nf + 31) / 32;
+      if (sd_m == 1 && td_m == 1 && m2l_sweep_supported(op.nfc)) {
+        const int nf = op.nfc, ftiles = (nf + 31) / 32;
         std::vector<T> kt((size_t)ftiles * 343 * 32 * 2, T(0));
         for (int ft = 0; ft < ftiles; ft++)
           for (int o = 0; o < 343; o++)
@@ -303,11 +303,11 @@ struct Impl : ImplBase {
         if (mark[g]) fwdn.push_back(g);
       m2l = make_list(work, {}, ptr, idx);
       fwd = make_list(fwdn, {});
-      effval = dalloc<T>((size_t)nn * td_m * op.nfreq * 2);
+      effval = dalloc<T>((size_t)nn * td_m * op.nfc * 2);
       // nn + 8 blocks: nodes outside every V list keep a zero spectrum, and the
       // 8 blocks from index nn on stand for an absent colleague (parent-pair form)
-      spectra = dalloc<T>((size_t)(nn + 8) * sd_m * op.nfreq * 2);
-      KCHECK(cudaMemset(spectra, 0, sizeof(T) * (size_t)(nn + 8) * sd_m * op.nfreq * 2));
+      spectra = dalloc<T>((size_t)(nn + 8) * sd_m * op.nfc * 2);
+      KCHECK(cudaMemset(spectra, 0, sizeof(T) * (size_t)(nn + 8) * sd_m * op.nfc * 2));
       counters_v = (double)idx.size();
       if (ktiles) build_pairs(work);
       counters_fwd = (double)fwdn.size();
@@ -363,6 +363,9 @@ struct Impl : ImplBase {
     geom.n = op.n;
     geom.nh = op.nh;
     geom.nfreq = op.nfreq;
+    geom.nfc = op.nfc;
+    geom.fc2f = upload(op.fc2f);
+    geom.ff2c = upload(op.ff2c);
     geom.nsurf = nsurf;
     geom.surf_ijk = upload(op.surf_ijk);
     geom.sd = sd_m;
@@ -569,7 +572,7 @@ struct Impl : ImplBase {
         launch_m2l_forward<T>(geom, supeden, fwd.work, fwd.n, d_depth, spectra, st);
         if (prof && r == 0) KCHECK(cudaEventRecord(ev[7], st));
         if (pairs_n > 0)
-          launch_m2l_hadamard_sweep<T>(op.nfreq, ktiles, spectra, pairs_n, pairs_chd, pairs_coll, pairs_mask, effval,
+          launch_m2l_hadamard_sweep<T>(op.nfc, ktiles, spectra, pairs_n, pairs_chd, pairs_coll, pairs_mask, effval,
                                        tr.nnodes, d_status, num_sms, st);
         else
           launch_m2l_hadamard<T>(geom, khat, spectra, m2l.work, m2l.n, m2l.ptr, m2l.idx, d_path, effval, st);

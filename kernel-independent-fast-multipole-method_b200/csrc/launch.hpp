@@ -96,6 +96,9 @@ void split_tf32(int M, int K, const double* A, std::vector<float>* hi, std::vect
 // fmm3d/matmgnt3d.cpp:223-361).
 struct M2LGeom {
   int np = 0, n = 0, nh = 0, nfreq = 0, nsurf = 0;
+  int nfc = 0;                // stored (Hermitian-canonical) frequencies per spectrum
+  const int* fc2f = nullptr;  // device: compact -> full frequency index
+  const int* ff2c = nullptr;  // device: full -> compact c, or -c-1 for conj(compact c)
   const int* surf_ijk = nullptr;  // device, 3 per surface point
   int sd = 1, td = 1;
   int deg[4] = {0, 0, 0, 0};

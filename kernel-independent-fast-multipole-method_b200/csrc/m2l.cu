@@ -12,6 +12,12 @@
 //             points only.
 // The kernel spectra are computed once on the host (operators.cpp) with the
 // same sign convention w = exp(-2 pi i / n) and already carry 1/n^3.
+// Spectra are stored Hermitian-compacted: of the kx = 0 and kx = n/2 planes,
+// which a real grid's half spectrum repeats as X(kx,-ky,-kz) = conj X(kx,ky,kz),
+// only the canonical half is kept (4 np^3 + 4 values instead of 4 np^2 (np+1);
+// 868 of 1008 at np = 6).  The products K X keep the symmetry, so the
+// forward pass computes, the Hadamard pass multiplies and the inverse pass
+// reads back (conjugating the mirrored half) only the independent values.
 // Density and potential grids use indices [0, np) per axis; the reference's
 // np/2 shift (matmgnt3d.cpp:256) cancels between embedding and extraction.
 #include <algorithm>
@@ -65,7 +71,7 @@ __global__ void __launch_bounds__(256) k_m2l_fwd_warp(M2LGeom g, const T* __rest
   extern __shared__ __align__(16) unsigned char smem_raw[];
   // NP > 0: compile-time sizes (constant divisors, unrolled sums); NP = 0: any np
   const int np = NP > 0 ? NP : g.np, n = NP > 0 ? 2 * NP : g.n, nh = NP > 0 ? NP + 1 : g.nh;
-  const int nf = NP > 0 ? 4 * NP * NP * (NP + 1) : g.nfreq;
+  const int nfc = NP > 0 ? 4 * NP * NP * NP + 4 : g.nfc;
   const int nsurf = NP > 0 ? NP * NP * NP - (NP - 2) * (NP - 2) * (NP - 2) : g.nsurf;
   Cpx<T>* W2 = reinterpret_cast<Cpx<T>*>(smem_raw);
   fill_w2(W2, n);
@@ -116,8 +122,9 @@ __global__ void __launch_bounds__(256) k_m2l_fwd_warp(M2LGeom g, const T* __rest
         Bm[e].im = im;
       }
       __syncwarp();
-      Cpx<T>* out = reinterpret_cast<Cpx<T>*>(spectra + ((size_t)node * g.sd + s) * nf * 2);
-      for (int e = lane; e < nf; e += 32) {  // z pass
+      Cpx<T>* out = reinterpret_cast<Cpx<T>*>(spectra + ((size_t)node * g.sd + s) * nfc * 2);
+      for (int c = lane; c < nfc; c += 32) {  // z pass, at the canonical frequencies only
+        const int e = g.fc2f[c];
         int kxy = e % (n * nh), kz = e / (n * nh);
         Cpx<T> r;
         r.re = r.im = T(0);
@@ -128,7 +135,7 @@ __global__ void __launch_bounds__(256) k_m2l_fwd_warp(M2LGeom g, const T* __rest
           r.re += b.re * t.re - b.im * t.im;
           r.im += b.re * t.im + b.im * t.re;
         }
-        out[e] = r;
+        out[c] = r;
       }
       __syncwarp();
     }
@@ -143,6 +150,7 @@ __global__ void __launch_bounds__(256) k_m2l_inv_warp(M2LGeom g, const T* __rest
   // NP > 0: compile-time sizes (constant divisors, unrolled sums); NP = 0: any np
   const int np = NP > 0 ? NP : g.np, n = NP > 0 ? 2 * NP : g.n, nh = NP > 0 ? NP + 1 : g.nh;
   const int nf = NP > 0 ? 4 * NP * NP * (NP + 1) : g.nfreq;
+  const int nfc = NP > 0 ? 4 * NP * NP * NP + 4 : g.nfc;
   const int nsurf = NP > 0 ? NP * NP * NP - (NP - 2) * (NP - 2) * (NP - 2) : g.nsurf;
   Cpx<T>* W2 = reinterpret_cast<Cpx<T>*>(smem_raw);
   fill_w2(W2, n);
@@ -156,8 +164,13 @@ __global__ void __launch_bounds__(256) k_m2l_inv_warp(M2LGeom g, const T* __rest
     const int node = work[wi];
     T* dst = tdncval + (size_t)node * nsurf * g.td;
     for (int t = 0; t < g.td; t++) {
-      const Cpx<T>* src = reinterpret_cast<const Cpx<T>*>(effval + ((size_t)node * g.td + t) * nf * 2);
-      for (int e = lane; e < nf; e += 32) Y[e] = src[e];
+      const Cpx<T>* src = reinterpret_cast<const Cpx<T>*>(effval + ((size_t)node * g.td + t) * nfc * 2);
+      for (int e = lane; e < nf; e += 32) {  // full half spectrum from the canonical values
+        const int m = g.ff2c[e];
+        Cpx<T> v = src[m >= 0 ? m : -m - 1];
+        if (m < 0) v.im = -v.im;
+        Y[e] = v;
+      }
       __syncwarp();
       for (int e = lane; e < np * n * nh; e += 32) {  // z pass (inverse), k < np
         int kxy = e % (n * nh), k = e / (n * nh);
@@ -217,7 +230,7 @@ __global__ void __launch_bounds__(FFT_THREADS) k_m2l_had(M2LGeom g, const T* __r
   __shared__ int vs[VMAX], vo[VMAX];
   const int wi = blockIdx.x;
   const int t = work[wi];
-  const int nf = g.nfreq;
+  const int nf = g.nfc;  // canonical frequencies only
   const int64_t b = vptr[wi];
   const int cnt = (int)(vptr[wi + 1] - b);
   const int tp0 = path[3 * t], tp1 = path[3 * t + 1], tp2 = path[3 * t + 2];
@@ -366,6 +379,111 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned parity)
   return false;
 }
 
+// The work of one frequency tile for one warp: claim QPT target parents at a
+// time from *claim until the CTA's slice [.., qend) is exhausted.
+template <typename T, int NF, int QPT>
+__device__ __forceinline__ void sweep_tile(const Cpx<T>* __restrict__ Ks, const Cpx<T>* __restrict__ spectra,
+                                           int* claim, int qend, int f, const int* __restrict__ qchd,
+                                           const int* __restrict__ coll, const unsigned char* __restrict__ mask,
+                                           Cpx<T>* __restrict__ effval, int zero_node) {
+  const int lane = threadIdx.x & 31;
+  const int fl = min(f, NF - 1);  // lanes past NF load a valid spectrum and store nothing
+  while (true) {
+    int q0 = 0;
+    if (lane == 0) q0 = atomicAdd(claim, QPT);
+    q0 = __shfl_sync(0xffffffffu, q0, 0);
+    if (q0 >= qend) break;
+    T ar[QPT][8], ai[QPT][8];
+#pragma unroll
+    for (int q = 0; q < QPT; q++)
+#pragma unroll
+      for (int i = 0; i < 8; i++) ar[q][i] = ai[q][i] = T(0);
+    const int* cq[QPT];
+#pragma unroll
+    for (int q = 0; q < QPT; q++) cq[q] = coll + (size_t)min(q0 + q, qend - 1) * 26;
+    int nb[QPT];
+    T nxr[QPT][8], nxi[QPT][8];
+#pragma unroll
+    for (int q = 0; q < QPT; q++) {
+      nb[q] = (q0 + q < qend) ? cq[q][0] : zero_node;
+      const Cpx<T>* X = spectra + (size_t)nb[q] * NF + fl;
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        Cpx<T> x = X[j * NF];
+        nxr[q][j] = x.re;
+        nxi[q][j] = x.im;
+      }
+    }
+    for (int dir = 0; dir < 26; dir++) {
+      T xr[QPT][8], xi[QPT][8];
+      bool any = false;
+#pragma unroll
+      for (int q = 0; q < QPT; q++) {
+        any |= nb[q] != zero_node;
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+          xr[q][j] = nxr[q][j];
+          xi[q][j] = nxi[q][j];
+        }
+      }
+      if (dir + 1 < 26) {
+#pragma unroll
+        for (int q = 0; q < QPT; q++) {
+          nb[q] = (q0 + q < qend) ? cq[q][dir + 1] : zero_node;
+          const Cpx<T>* X = spectra + (size_t)nb[q] * NF + fl;
+#pragma unroll
+          for (int j = 0; j < 8; j++) {
+            Cpx<T> x = X[j * NF];
+            nxr[q][j] = x.re;
+            nxi[q][j] = x.im;
+          }
+        }
+      }
+      if (!any) continue;
+      // offset of child j of P from child i of Q: 2*dir + oct(j) - oct(i); the
+      // adjacent pairs (|offset| <= 1) read the zero rows of the tile
+      const Cpx<T>* Kd = Ks + c_dir_base[dir] * 32 + lane;
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+          const int cij = (((j >> 2) & 1) - ((i >> 2) & 1)) * 49 + (((j >> 1) & 1) - ((i >> 1) & 1)) * 7 +
+                          ((j & 1) - (i & 1));
+          const Cpx<T> k = Kd[cij * 32];
+#pragma unroll
+          for (int q = 0; q < QPT; q++) {
+            ar[q][i] += k.re * xr[q][j] - k.im * xi[q][j];
+            ai[q][i] += k.re * xi[q][j] + k.im * xr[q][j];
+          }
+        }
+      }
+    }
+    if (f < NF) {
+#pragma unroll
+      for (int q = 0; q < QPT; q++) {
+        if (q0 + q >= qend) continue;
+        const int c0 = qchd[q0 + q];
+        const unsigned m = mask[q0 + q];
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+          if (!((m >> i) & 1)) continue;
+          Cpx<T> y;
+          y.re = ar[q][i];
+          y.im = ai[q][i];
+          effval[(size_t)(c0 + i) * NF + f] = y;
+        }
+      }
+    }
+  }
+}
+
+// NBUF = 2 (FP32): no CTA-wide barrier inside the sweep.  Each warp walks the
+// frequency tiles on its own; the last warp to finish a tile (a shared
+// counter) resets that buffer's claim counter and issues the copy of the tile
+// two ahead into it, so warps drift apart by at most one tile.  The copy's
+// mbarrier arrive releases the reset to the warps that wait on that buffer.
+// NBUF = 1 (FP64, one 176 KB tile): the tile is reloaded between two CTA
+// barriers.
 template <typename T, int NF, int QPT, int NTHR, int NBUF>
 __global__ void __launch_bounds__(NTHR) k_m2l_had_sweep(const Cpx<T>* __restrict__ ktiles,
                                                        const Cpx<T>* __restrict__ spectra, int nq,
@@ -376,130 +494,64 @@ __global__ void __launch_bounds__(NTHR) k_m2l_had_sweep(const Cpx<T>* __restrict
   constexpr int TILE = 343 * 32;
   constexpr unsigned TILE_BYTES = TILE * sizeof(Cpx<T>);
   constexpr int FTILES = (NF + 31) / 32;
+  constexpr int NW = NTHR / 32;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Cpx<T>* Kbuf = reinterpret_cast<Cpx<T>*>(smem_raw);  // NBUF x [343][32]
   __shared__ __align__(8) unsigned long long bars[NBUF];
-  __shared__ int next_q;  // next unclaimed group of the CTA's slice, per frequency tile
+  __shared__ int claim[NBUF], done_cnt[NBUF];
   const int lane = threadIdx.x & 31;
   const int per_cta = (nq + gridDim.x - 1) / gridDim.x;
   const int qbeg = blockIdx.x * per_cta;
   const int qend = min(nq, qbeg + per_cta);
   if (threadIdx.x == 0) {
-    for (int b = 0; b < NBUF; b++) mbar_init(smem_addr(&bars[b]), 1);
+    for (int b = 0; b < NBUF; b++) {
+      mbar_init(smem_addr(&bars[b]), 1);
+      claim[b] = qbeg;
+      done_cnt[b] = 0;
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    if (NBUF == 2) bulk_load(smem_addr(Kbuf), ktiles, TILE_BYTES, smem_addr(&bars[0]));
+    if (NBUF == 2) {
+      bulk_load(smem_addr(Kbuf), ktiles, TILE_BYTES, smem_addr(&bars[0]));
+      if (FTILES > 1) bulk_load(smem_addr(Kbuf + TILE), ktiles + TILE, TILE_BYTES, smem_addr(&bars[1]));
+    }
   }
   __syncthreads();
-  for (int ft = 0; ft < FTILES; ft++) {
-    const int buf = NBUF == 2 ? (ft & 1) : 0;
-    const unsigned parity = NBUF == 2 ? ((ft >> 1) & 1) : (ft & 1);
-    if (threadIdx.x == 0) {
-      next_q = qbeg;
-      // the buffer written here was last read in tile ft-1, which every warp
-      // has finished (barrier at the end of the previous iteration)
-      if (NBUF == 2 && ft + 1 < FTILES)
-        bulk_load(smem_addr(Kbuf + (size_t)((ft + 1) & 1) * TILE), ktiles + (size_t)(ft + 1) * TILE, TILE_BYTES,
-                  smem_addr(&bars[(ft + 1) & 1]));
-      if (NBUF == 1) bulk_load(smem_addr(Kbuf), ktiles + (size_t)ft * TILE, TILE_BYTES, smem_addr(&bars[0]));
-    }
-    __syncthreads();
-    const bool ok = mbar_wait_bounded(smem_addr(&bars[buf]), parity);
-    if (__syncthreads_or(!ok)) {
-      if (threadIdx.x == 0) atomicOr(status, 1);
-      return;
-    }
-    const Cpx<T>* Ks = Kbuf + (size_t)buf * TILE;
-    const int f = ft * 32 + lane;
-    const int fl = min(f, NF - 1);  // lanes past NF load a valid spectrum and store nothing
-    // warps claim QPT target parents at a time, so they finish the tile together
-    while (true) {
-      int q0 = 0;
-      if (lane == 0) q0 = atomicAdd(&next_q, QPT);
-      q0 = __shfl_sync(0xffffffffu, q0, 0);
-      if (q0 >= qend) break;
-      T ar[QPT][8], ai[QPT][8];
-#pragma unroll
-      for (int q = 0; q < QPT; q++)
-#pragma unroll
-        for (int i = 0; i < 8; i++) ar[q][i] = ai[q][i] = T(0);
-      const int* cq[QPT];
-#pragma unroll
-      for (int q = 0; q < QPT; q++) cq[q] = coll + (size_t)min(q0 + q, qend - 1) * 26;
-      int nb[QPT];
-      T nxr[QPT][8], nxi[QPT][8];
-#pragma unroll
-      for (int q = 0; q < QPT; q++) {
-        nb[q] = (q0 + q < qend) ? cq[q][0] : zero_node;
-        const Cpx<T>* X = spectra + (size_t)nb[q] * NF + fl;
-#pragma unroll
-        for (int j = 0; j < 8; j++) {
-          Cpx<T> x = X[j * NF];
-          nxr[q][j] = x.re;
-          nxi[q][j] = x.im;
+  if constexpr (NBUF == 2) {
+    for (int ft = 0; ft < FTILES; ft++) {
+      const int b = ft & 1;
+      const bool ok = mbar_wait_bounded(smem_addr(&bars[b]), (ft >> 1) & 1);
+      if (!ok) {  // the warp stops; the others then time out on the tiles it never releases
+        if (lane == 0) atomicOr(status, 1);
+        return;
+      }
+      sweep_tile<T, NF, QPT>(Kbuf + (size_t)b * TILE, spectra, &claim[b], qend, ft * 32 + lane, qchd, coll, mask,
+                             effval, zero_node);
+      if (lane == 0) {
+        if (atomicAdd(&done_cnt[b], 1) == NW - 1) {  // the last warp out of tile ft
+          done_cnt[b] = 0;
+          claim[b] = qbeg;
+          if (ft + 2 < FTILES)
+            bulk_load(smem_addr(Kbuf + (size_t)b * TILE), ktiles + (size_t)(ft + 2) * TILE, TILE_BYTES,
+                      smem_addr(&bars[b]));
         }
       }
-      for (int dir = 0; dir < 26; dir++) {
-        T xr[QPT][8], xi[QPT][8];
-        bool any = false;
-#pragma unroll
-        for (int q = 0; q < QPT; q++) {
-          any |= nb[q] != zero_node;
-#pragma unroll
-          for (int j = 0; j < 8; j++) {
-            xr[q][j] = nxr[q][j];
-            xi[q][j] = nxi[q][j];
-          }
-        }
-        if (dir + 1 < 26) {
-#pragma unroll
-          for (int q = 0; q < QPT; q++) {
-            nb[q] = (q0 + q < qend) ? cq[q][dir + 1] : zero_node;
-            const Cpx<T>* X = spectra + (size_t)nb[q] * NF + fl;
-#pragma unroll
-            for (int j = 0; j < 8; j++) {
-              Cpx<T> x = X[j * NF];
-              nxr[q][j] = x.re;
-              nxi[q][j] = x.im;
-            }
-          }
-        }
-        if (!any) continue;
-        // offset of child j of P from child i of Q: 2*dir + oct(j) - oct(i); the
-        // adjacent pairs (|offset| <= 1) read the zero rows of the tile
-        const Cpx<T>* Kd = Ks + c_dir_base[dir] * 32 + lane;
-#pragma unroll
-        for (int j = 0; j < 8; j++) {
-#pragma unroll
-          for (int i = 0; i < 8; i++) {
-            const int cij = (((j >> 2) & 1) - ((i >> 2) & 1)) * 49 + (((j >> 1) & 1) - ((i >> 1) & 1)) * 7 +
-                            ((j & 1) - (i & 1));
-            const Cpx<T> k = Kd[cij * 32];
-#pragma unroll
-            for (int q = 0; q < QPT; q++) {
-              ar[q][i] += k.re * xr[q][j] - k.im * xi[q][j];
-              ai[q][i] += k.re * xi[q][j] + k.im * xr[q][j];
-            }
-          }
-        }
-      }
-      if (f < NF) {
-#pragma unroll
-        for (int q = 0; q < QPT; q++) {
-          if (q0 + q >= qend) continue;
-          const int c0 = qchd[q0 + q];
-          const unsigned m = mask[q0 + q];
-#pragma unroll
-          for (int i = 0; i < 8; i++) {
-            if (!((m >> i) & 1)) continue;
-            Cpx<T> y;
-            y.re = ar[q][i];
-            y.im = ai[q][i];
-            effval[(size_t)(c0 + i) * NF + f] = y;
-          }
-        }
-      }
+      __syncwarp();
     }
-    __syncthreads();
+  } else {
+    for (int ft = 0; ft < FTILES; ft++) {
+      if (threadIdx.x == 0) {
+        claim[0] = qbeg;
+        bulk_load(smem_addr(Kbuf), ktiles + (size_t)ft * TILE, TILE_BYTES, smem_addr(&bars[0]));
+      }
+      __syncthreads();
+      const bool ok = mbar_wait_bounded(smem_addr(&bars[0]), ft & 1);
+      if (__syncthreads_or(!ok)) {
+        if (threadIdx.x == 0) atomicOr(status, 1);
+        return;
+      }
+      sweep_tile<T, NF, QPT>(Kbuf, spectra, &claim[0], qend, ft * 32 + lane, qchd, coll, mask, effval, zero_node);
+      __syncthreads();
+    }
   }
 }
 
@@ -521,19 +573,19 @@ void sweep_launch(const T* ktiles, const T* spectra, int nq, const int* qchd, co
 
 }  // namespace
 
-bool m2l_sweep_supported(int nf) { return nf == 320 || nf == 1008 || nf == 2304; }
+bool m2l_sweep_supported(int nf) { return nf == 260 || nf == 868 || nf == 2052; }
 
 template <typename T>
 void launch_m2l_hadamard_sweep(int nf, const T* ktiles, const T* spectra, int nq, const int* qchd, const int* coll,
                                const unsigned char* mask, T* effval, int zero_node, int* status, int num_sms,
                                cudaStream_t st) {
   if (nq <= 0) return;
-  if (nf == 1008)
-    sweep_launch<T, 1008>(ktiles, spectra, nq, qchd, coll, mask, effval, zero_node, status, num_sms, st);
-  else if (nf == 320)
-    sweep_launch<T, 320>(ktiles, spectra, nq, qchd, coll, mask, effval, zero_node, status, num_sms, st);
-  else if (nf == 2304)
-    sweep_launch<T, 2304>(ktiles, spectra, nq, qchd, coll, mask, effval, zero_node, status, num_sms, st);
+  if (nf == 868)
+    sweep_launch<T, 868>(ktiles, spectra, nq, qchd, coll, mask, effval, zero_node, status, num_sms, st);
+  else if (nf == 260)
+    sweep_launch<T, 260>(ktiles, spectra, nq, qchd, coll, mask, effval, zero_node, status, num_sms, st);
+  else if (nf == 2052)
+    sweep_launch<T, 2052>(ktiles, spectra, nq, qchd, coll, mask, effval, zero_node, status, num_sms, st);
 }
 
 #define KIFMM_INST(T)                                                                                             \

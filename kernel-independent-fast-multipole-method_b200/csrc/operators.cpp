@@ -423,9 +423,34 @@ std::shared_ptr<Operators> build_operators(const KernelDesc& mm, int np, int nth
   // M2L spectra (fmm3d/matmgnt3d.cpp:307-325): kernel sampled at
   // reg(g) - 2*idx with reg(g) = wrap(g)*step, wrap(g) = g < np ? g : g - n,
   // transformed with w = exp(-2 pi i / n); kx halved; scaled by 1/n^3.
-  const int n = o.n, nh = o.nh, nf = o.nfreq;
+  const int n = o.n, nh = o.nh;
   const double step = 2.0 / (np - 1);
-  o.m2l.assign((size_t)343 * td * sd * nf, std::complex<double>(0.0, 0.0));
+  // Hermitian compaction: a real grid's half spectrum (kx < nh) repeats its
+  // kx = 0 and kx = n/2 planes as X(kx,-ky,-kz) = conj X(kx,ky,kz); only the
+  // canonical member of each pair, (kz,ky) <= (-kz,-ky) mod n, is kept.
+  o.ff2c.assign(o.nfreq, 0);
+  o.fc2f.clear();
+  for (int kz = 0; kz < n; kz++)
+    for (int ky = 0; ky < n; ky++)
+      for (int kx = 0; kx < nh; kx++) {
+        const int f = (kz * n + ky) * nh + kx;
+        const int mz = (n - kz) % n, my = (n - ky) % n;
+        const bool edge = kx == 0 || 2 * kx == n;
+        if (!edge || kz < mz || (kz == mz && ky <= my)) {
+          o.ff2c[f] = (int)o.fc2f.size();
+          o.fc2f.push_back(f);
+        }
+      }
+  o.nfc = (int)o.fc2f.size();
+  for (int kz = 0; kz < n; kz++)
+    for (int ky = 0; ky < n; ky++)
+      for (int kx : {0, n / 2}) {
+        const int f = (kz * n + ky) * nh + kx;
+        const int mz = (n - kz) % n, my = (n - ky) % n;
+        if (!(kz < mz || (kz == mz && ky <= my))) o.ff2c[f] = -o.ff2c[(mz * n + my) * nh + kx] - 1;
+      }
+  const int nfc = o.nfc;
+  o.m2l.assign((size_t)343 * td * sd * nfc, std::complex<double>(0.0, 0.0));
   std::vector<std::complex<double>> w(n);
   for (int j = 0; j < n; j++) w[j] = std::polar(1.0, -2.0 * M_PI * j / n);
   const double scale = 1.0 / ((double)n * n * n);
@@ -466,15 +491,14 @@ std::shared_ptr<Operators> build_operators(const KernelDesc& mm, int np, int nth
             for (int gy = 0; gy < n; gy++) s += A[((size_t)gz * n + gy) * nh + kx] * w[(gy * ky) % n];
             B[((size_t)gz * n + ky) * nh + kx] = s;
           }
-      // z pass: f = (kz*n + ky)*nh + kx
-      std::complex<double>* dst = &o.m2l[((size_t)oidx * td * sd + e) * nf];
-      for (int kz = 0; kz < n; kz++)
-        for (int ky = 0; ky < n; ky++)
-          for (int kx = 0; kx < nh; kx++) {
-            std::complex<double> s(0, 0);
-            for (int gz = 0; gz < n; gz++) s += B[((size_t)gz * n + ky) * nh + kx] * w[(gz * kz) % n];
-            dst[((size_t)kz * n + ky) * nh + kx] = s * scale;
-          }
+      // z pass at the canonical frequencies, f = (kz*n + ky)*nh + kx
+      std::complex<double>* dst = &o.m2l[((size_t)oidx * td * sd + e) * nfc];
+      for (int c = 0; c < nfc; c++) {
+        const int f = o.fc2f[c], kx = f % nh, ky = (f / nh) % n, kz = f / (nh * n);
+        std::complex<double> s(0, 0);
+        for (int gz = 0; gz < n; gz++) s += B[((size_t)gz * n + ky) * nh + kx] * w[(gz * kz) % n];
+        dst[c] = s * scale;
+      }
     }
   });
   return op;

@@ -56,10 +56,13 @@ struct Operators {
   int nuc = 0;            // |UC| = (np+2)^3 - np^3
   int n = 0, nh = 0;      // FFT grid 2np, halved axis n/2+1
   int nfreq = 0;          // n*n*nh
+  int nfc = 0;            // independent (Hermitian-canonical) frequencies, 4 np^3 + 4
+  std::vector<int> fc2f;  // compact -> full frequency index
+  std::vector<int> ff2c;  // full -> compact index c, or -c-1 where the value is conj(compact c)
   std::vector<int> deg;   // per sd
   std::vector<double> ue, uc, de, dc;   // unit grids (3 per point), radii 1, 3, 3, 1
   std::vector<int> surf_ijk;            // (i,j,k) grid index of each np-surface point
-  std::vector<std::complex<double>> m2l;  // [343 offsets][td][sd][nfreq], scaled by 1/n^3
+  std::vector<std::complex<double>> m2l;  // [343 offsets][td][sd][nfc], scaled by 1/n^3
   // Surface contractions in factored form.  UC2UE = pinv(K(UC <- UE)) =
   // up_V * up_W and DC2DE = pinv(K(DC <- DE)) = dn_V * dn_W, V with orthonormal
   // columns and W = Sigma^-1 U^T.  The pseudo-inverses' entries reach
