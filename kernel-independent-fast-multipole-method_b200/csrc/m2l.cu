@@ -58,6 +58,12 @@ __host__ __device__ inline size_t fwd_warp_bytes(int np, int n, int nh) {
          align16(sizeof(Cpx<T>) * np * n * nh);
 }
 
+// register-blocked inverse: Bm (np x n x nh) and A (np x np x nh) per warp
+template <typename T>
+__host__ __device__ inline size_t inv_rb_warp_bytes(int np, int n, int nh) {
+  return align16(sizeof(Cpx<T>) * np * n * nh) + align16(sizeof(Cpx<T>) * np * np * nh);
+}
+
 template <typename T>
 __host__ __device__ inline size_t inv_warp_bytes(int np, int n, int nh) {
   return align16(sizeof(Cpx<T>) * n * n * nh) + align16(sizeof(Cpx<T>) * np * n * nh) +
@@ -274,6 +280,269 @@ __global__ void __launch_bounds__(FFT_THREADS) k_m2l_had(M2LGeom g, const T* __r
   }
 }
 
+// ---------------------------------------------------------------------------
+// Register-blocked transforms for np = 4, 6, 8.  Each lane owns one line of a
+// pass, keeps that line's np (or n) inputs in registers and produces every
+// output of the line, so a shared-memory value feeds a whole row of complex
+// multiply-adds instead of one.  The twiddle factors are compile-time
+// constants (tw_re / tw_im below), folded into the multiply-adds.
+
+// cos and sin on |r| <= pi/4 by their Taylor series (10 terms: below 1e-20)
+__host__ __device__ constexpr double taylor_sin(double r) {
+  double r2 = r * r, t = r, s = r;
+  for (int k = 1; k <= 10; k++) {
+    t *= -r2 / ((2.0 * k) * (2.0 * k + 1.0));
+    s += t;
+  }
+  return s;
+}
+__host__ __device__ constexpr double taylor_cos(double r) {
+  double r2 = r * r, t = 1.0, s = 1.0;
+  for (int k = 1; k <= 10; k++) {
+    t *= -r2 / ((2.0 * k - 1.0) * (2.0 * k));
+    s += t;
+  }
+  return s;
+}
+// w^m = exp(-2 pi i m / n): the angle 2 pi m / n is split into q quarter turns
+// plus a remainder r, |r| <= pi/4, both exact in m and n
+__host__ __device__ constexpr double tw_re(int m, int n) {
+  m %= n;
+  const int q = (8 * m + n) / (2 * n);
+  const double r = 1.5707963267948966 * (double)(4 * m - q * n) / (double)n;
+  const int o = q & 3;
+  return o == 0 ? taylor_cos(r) : o == 1 ? -taylor_sin(r) : o == 2 ? -taylor_cos(r) : taylor_sin(r);
+}
+__host__ __device__ constexpr double tw_im(int m, int n) {
+  m %= n;
+  const int q = (8 * m + n) / (2 * n);
+  const double r = 1.5707963267948966 * (double)(4 * m - q * n) / (double)n;
+  const int o = q & 3;
+  const double s = o == 0 ? taylor_sin(r) : o == 1 ? taylor_cos(r) : o == 2 ? -taylor_sin(r) : -taylor_cos(r);
+  return -s;
+}
+
+// twiddle tables for n = 8, 12, 16, statically initialised from tw_re / tw_im;
+// indexed with compile-time offsets they are constant-bank operands
+#define KIFMM_TW16(F, n)                                                                                         \
+  {F(0, n), F(1, n), F(2, n), F(3, n), F(4, n), F(5, n), F(6, n), F(7, n), F(8, n), F(9, n), F(10, n), F(11, n), \
+   F(12, n), F(13, n), F(14, n), F(15, n)}
+#define KIFMM_TWSET(F) {KIFMM_TW16(F, 8), KIFMM_TW16(F, 12), KIFMM_TW16(F, 16)}
+#define KIFMM_FRE(m, n) (float)tw_re(m, n)
+#define KIFMM_FIM(m, n) (float)tw_im(m, n)
+#define KIFMM_DRE(m, n) tw_re(m, n)
+#define KIFMM_DIM(m, n) tw_im(m, n)
+__constant__ float c_twf_re[3][16] = KIFMM_TWSET(KIFMM_FRE);
+__constant__ float c_twf_im[3][16] = KIFMM_TWSET(KIFMM_FIM);
+__constant__ double c_twd_re[3][16] = KIFMM_TWSET(KIFMM_DRE);
+__constant__ double c_twd_im[3][16] = KIFMM_TWSET(KIFMM_DIM);
+#undef KIFMM_FRE
+#undef KIFMM_FIM
+#undef KIFMM_DRE
+#undef KIFMM_DIM
+#undef KIFMM_TWSET
+#undef KIFMM_TW16
+
+template <typename T, int N>
+__device__ __forceinline__ T twr(int m) {
+  constexpr int t = N == 8 ? 0 : N == 12 ? 1 : 2;
+  if constexpr (sizeof(T) == 4)
+    return c_twf_re[t][m % N];
+  else
+    return c_twd_re[t][m % N];
+}
+template <typename T, int N>
+__device__ __forceinline__ T twi(int m) {
+  constexpr int t = N == 8 ? 0 : N == 12 ? 1 : 2;
+  if constexpr (sizeof(T) == 4)
+    return c_twf_im[t][m % N];
+  else
+    return c_twd_im[t][m % N];
+}
+
+template <typename T, int NP>
+__global__ void __launch_bounds__(256) k_m2l_fwd_rb(M2LGeom g, const T* __restrict__ supeden,
+                                                    const int* __restrict__ nodes, int nwork,
+                                                    const int* __restrict__ depth, T* __restrict__ spectra) {
+  constexpr int N = 2 * NP, NH = NP + 1, NFC = 4 * NP * NP * NP + 4;
+  constexpr int NSURF = NP * NP * NP - (NP - 2) * (NP - 2) * (NP - 2);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpc = blockDim.x >> 5;
+  int* c_of = reinterpret_cast<int*>(smem_raw);  // full -> compact frequency index (< 0: not stored)
+  for (int e = threadIdx.x; e < N * N * NH; e += blockDim.x) c_of[e] = g.ff2c[e];
+  unsigned char* mine = smem_raw + align16(sizeof(int) * N * N * NH) + (size_t)warp * fwd_warp_bytes<T>(NP, N, NH);
+  T* xg = reinterpret_cast<T*>(mine);
+  Cpx<T>* A = reinterpret_cast<Cpx<T>*>(mine + align16(sizeof(T) * NP * NP * NP));
+  Cpx<T>* Bm = reinterpret_cast<Cpx<T>*>(reinterpret_cast<unsigned char*>(A) + align16(sizeof(Cpx<T>) * NP * NP * NH));
+  __syncthreads();
+  for (int wi = blockIdx.x * wpc + warp; wi < nwork; wi += gridDim.x * wpc) {
+    const int node = nodes[wi];
+    const int lvl = depth[node] + g.rootlvl;
+    const T* den = supeden + (size_t)node * NSURF * g.sd;
+    for (int s = 0; s < g.sd; s++) {
+      const T scale = (T)ldexp(1.0, lvl * g.deg[s]);  // plnden2effden scaling, matmgnt3d.cpp:228-235
+      for (int e = lane; e < NP * NP * NP; e += 32) xg[e] = T(0);
+      __syncwarp();
+      for (int k = lane; k < NSURF; k += 32) {
+        const int i = g.surf_ijk[3 * k], j = g.surf_ijk[3 * k + 1], kk = g.surf_ijk[3 * k + 2];
+        xg[(i * NP + j) * NP + kk] = den[(size_t)k * g.sd + s] * scale;
+      }
+      __syncwarp();
+      // x pass, lines (j, k): A[k][j][kx] = sum_i xg[i][j][k] w^(i kx)
+      for (int line = lane; line < NP * NP; line += 32) {
+        const int j = line % NP, k = line / NP;
+        T v[NP];
+#pragma unroll
+        for (int i = 0; i < NP; i++) v[i] = xg[(i * NP + j) * NP + k];
+#pragma unroll
+        for (int kx = 0; kx < NH; kx++) {
+          T re = 0, im = 0;
+#pragma unroll
+          for (int i = 0; i < NP; i++) {
+            re += v[i] * twr<T, N>(i * kx);
+            im += v[i] * twi<T, N>(i * kx);
+          }
+          A[(k * NP + j) * NH + kx] = Cpx<T>{re, im};
+        }
+      }
+      __syncwarp();
+      // y pass, lines (k, kx): Bm[k][ky][kx] = sum_j A[k][j][kx] w^(j ky)
+      for (int line = lane; line < NP * NH; line += 32) {
+        const int kx = line % NH, k = line / NH;
+        Cpx<T> a[NP];
+#pragma unroll
+        for (int j = 0; j < NP; j++) a[j] = A[(k * NP + j) * NH + kx];
+#pragma unroll
+        for (int ky = 0; ky < N; ky++) {
+          T re = 0, im = 0;
+#pragma unroll
+          for (int j = 0; j < NP; j++) {
+            const T c = twr<T, N>(j * ky), d = twi<T, N>(j * ky);
+            re += a[j].re * c - a[j].im * d;
+            im += a[j].re * d + a[j].im * c;
+          }
+          Bm[(k * N + ky) * NH + kx] = Cpx<T>{re, im};
+        }
+      }
+      __syncwarp();
+      // z pass, lines (ky, kx): spectrum[kz][ky][kx] = sum_k Bm[k][ky][kx] w^(k kz), canonical only
+      Cpx<T>* out = reinterpret_cast<Cpx<T>*>(spectra + ((size_t)node * g.sd + s) * NFC * 2);
+      for (int line = lane; line < N * NH; line += 32) {
+        const int kx = line % NH, ky = line / NH;
+        Cpx<T> b[NP];
+#pragma unroll
+        for (int k = 0; k < NP; k++) b[k] = Bm[(k * N + ky) * NH + kx];
+#pragma unroll
+        for (int kz = 0; kz < N; kz++) {
+          const int c = c_of[(kz * N + ky) * NH + kx];
+          if (c < 0) continue;
+          T re = 0, im = 0;
+#pragma unroll
+          for (int k = 0; k < NP; k++) {
+            const T cr = twr<T, N>(k * kz), ci = twi<T, N>(k * kz);
+            re += b[k].re * cr - b[k].im * ci;
+            im += b[k].re * ci + b[k].im * cr;
+          }
+          out[c] = Cpx<T>{re, im};
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+template <typename T, int NP>
+__global__ void __launch_bounds__(256) k_m2l_inv_rb(M2LGeom g, const T* __restrict__ effval,
+                                                    const int* __restrict__ work, int nwork,
+                                                    T* __restrict__ tdncval) {
+  constexpr int N = 2 * NP, NH = NP + 1, NFC = 4 * NP * NP * NP + 4;
+  constexpr int NSURF = NP * NP * NP - (NP - 2) * (NP - 2) * (NP - 2);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpc = blockDim.x >> 5;
+  int* c_of = reinterpret_cast<int*>(smem_raw);                      // full -> compact (< 0: conj of -c-1)
+  int* m_of = c_of + N * N * NH;                                     // grid point (i,j,k) -> surface index or -1
+  for (int e = threadIdx.x; e < N * N * NH; e += blockDim.x) c_of[e] = g.ff2c[e];
+  for (int e = threadIdx.x; e < NP * NP * NP; e += blockDim.x) m_of[e] = -1;
+  __syncthreads();
+  for (int m = threadIdx.x; m < NSURF; m += blockDim.x)
+    m_of[(g.surf_ijk[3 * m] * NP + g.surf_ijk[3 * m + 1]) * NP + g.surf_ijk[3 * m + 2]] = m;
+  unsigned char* mine =
+      smem_raw + align16(sizeof(int) * (N * N * NH + NP * NP * NP)) + (size_t)warp * inv_rb_warp_bytes<T>(NP, N, NH);
+  Cpx<T>* Bm = reinterpret_cast<Cpx<T>*>(mine);
+  Cpx<T>* A = reinterpret_cast<Cpx<T>*>(mine + align16(sizeof(Cpx<T>) * NP * N * NH));
+  __syncthreads();
+  for (int wi = blockIdx.x * wpc + warp; wi < nwork; wi += gridDim.x * wpc) {
+    const int node = work[wi];
+    T* dst = tdncval + (size_t)node * NSURF * g.td;
+    for (int t = 0; t < g.td; t++) {
+      const Cpx<T>* src = reinterpret_cast<const Cpx<T>*>(effval + ((size_t)node * g.td + t) * NFC * 2);
+      // z pass (inverse), lines (ky, kx): Bm[k][ky][kx] = sum_kz Y[kz][ky][kx] w^(-k kz), k < np
+      for (int line = lane; line < N * NH; line += 32) {
+        const int kx = line % NH, ky = line / NH;
+        Cpx<T> y[N];
+#pragma unroll
+        for (int kz = 0; kz < N; kz++) {
+          const int c = c_of[(kz * N + ky) * NH + kx];
+          Cpx<T> v = src[c >= 0 ? c : -c - 1];
+          if (c < 0) v.im = -v.im;
+          y[kz] = v;
+        }
+#pragma unroll
+        for (int k = 0; k < NP; k++) {
+          T re = 0, im = 0;
+#pragma unroll
+          for (int kz = 0; kz < N; kz++) {
+            const T cr = twr<T, N>(k * kz), ci = twi<T, N>(k * kz);
+            re += y[kz].re * cr + y[kz].im * ci;
+            im += y[kz].im * cr - y[kz].re * ci;
+          }
+          Bm[(k * N + ky) * NH + kx] = Cpx<T>{re, im};
+        }
+      }
+      __syncwarp();
+      // y pass (inverse), lines (k, kx): A[k][j][kx] = sum_ky Bm[k][ky][kx] w^(-j ky), j < np
+      for (int line = lane; line < NP * NH; line += 32) {
+        const int kx = line % NH, k = line / NH;
+        Cpx<T> b[N];
+#pragma unroll
+        for (int ky = 0; ky < N; ky++) b[ky] = Bm[(k * N + ky) * NH + kx];
+#pragma unroll
+        for (int j = 0; j < NP; j++) {
+          T re = 0, im = 0;
+#pragma unroll
+          for (int ky = 0; ky < N; ky++) {
+            const T cr = twr<T, N>(j * ky), ci = twi<T, N>(j * ky);
+            re += b[ky].re * cr + b[ky].im * ci;
+            im += b[ky].im * cr - b[ky].re * ci;
+          }
+          A[(k * NP + j) * NH + kx] = Cpx<T>{re, im};
+        }
+      }
+      __syncwarp();
+      // c2r along x, lines (j, k): x_i = Re(a_0) + (-1)^i Re(a_{n/2}) + 2 sum_{0<kx<n/2} Re(a_kx w^(-i kx)),
+      // kept at the surface points only
+      for (int line = lane; line < NP * NP; line += 32) {
+        const int j = line % NP, k = line / NP;
+        Cpx<T> a[NH];
+#pragma unroll
+        for (int kx = 0; kx < NH; kx++) a[kx] = A[(k * NP + j) * NH + kx];
+#pragma unroll
+        for (int i = 0; i < NP; i++) {
+          const int m = m_of[(i * NP + j) * NP + k];
+          if (m < 0) continue;
+          T acc = 0;
+#pragma unroll
+          for (int kx = 1; kx < NH - 1; kx++)
+            acc += a[kx].re * twr<T, N>(i * kx) + a[kx].im * twi<T, N>(i * kx);
+          const T v = a[0].re + ((i & 1) ? -a[NH - 1].re : a[NH - 1].re);
+          dst[(size_t)m * g.td + t] += v + T(2) * acc;
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
 }  // namespace
 
 template <typename T>
@@ -286,12 +555,18 @@ void launch_m2l_forward(const M2LGeom& g, const T* supeden, const int* nodes, in
   int wpc = (int)std::max<size_t>(1, std::min<size_t>(8, (200 * 1024 - head) / per_warp));
   size_t smem = head + per_warp * wpc;
   int grid = std::max(1, std::min((nn + wpc - 1) / wpc, 148 * 8));
-  auto kern = g.np == 6 ? k_m2l_fwd_warp<T, 6>
-              : g.np == 4 ? k_m2l_fwd_warp<T, 4>
-              : g.np == 8 ? k_m2l_fwd_warp<T, 8>
-                          : k_m2l_fwd_warp<T, 0>;
-  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  kern<<<grid, 32 * wpc, smem, st>>>(g, supeden, nodes, nn, depth, spectra);
+  if (g.np == 4 || g.np == 6 || g.np == 8) {
+    const size_t head_rb = align16(sizeof(int) * g.n * g.n * g.nh);
+    const int w = (int)std::max<size_t>(1, std::min<size_t>(8, (200 * 1024 - head_rb) / per_warp));
+    const size_t sm = head_rb + per_warp * w;
+    const int gr = std::max(1, std::min((nn + w - 1) / w, 148 * 8));
+    auto kern = g.np == 6 ? k_m2l_fwd_rb<T, 6> : g.np == 4 ? k_m2l_fwd_rb<T, 4> : k_m2l_fwd_rb<T, 8>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    kern<<<gr, 32 * w, sm, st>>>(g, supeden, nodes, nn, depth, spectra);
+    return;
+  }
+  cudaFuncSetAttribute(k_m2l_fwd_warp<T, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_m2l_fwd_warp<T, 0><<<grid, 32 * wpc, smem, st>>>(g, supeden, nodes, nn, depth, spectra);
 }
 
 template <typename T>
@@ -314,12 +589,19 @@ void launch_m2l_inverse(const M2LGeom& g, const T* effval, const int* work, int 
   int wpc = (int)std::max<size_t>(1, std::min<size_t>(8, (200 * 1024 - head) / per_warp));
   size_t smem = head + per_warp * wpc;
   int grid = std::max(1, std::min((nwork + wpc - 1) / wpc, 148 * 8));
-  auto kern = g.np == 6 ? k_m2l_inv_warp<T, 6>
-              : g.np == 4 ? k_m2l_inv_warp<T, 4>
-              : g.np == 8 ? k_m2l_inv_warp<T, 8>
-                          : k_m2l_inv_warp<T, 0>;
-  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  kern<<<grid, 32 * wpc, smem, st>>>(g, effval, work, nwork, tdncval);
+  if (g.np == 4 || g.np == 6 || g.np == 8) {
+    const size_t per_rb = inv_rb_warp_bytes<T>(g.np, g.n, g.nh);
+    const size_t head_rb = align16(sizeof(int) * (g.n * g.n * g.nh + g.np * g.np * g.np));
+    const int w = (int)std::max<size_t>(1, std::min<size_t>(8, (200 * 1024 - head_rb) / per_rb));
+    const size_t sm = head_rb + per_rb * w;
+    const int gr = std::max(1, std::min((nwork + w - 1) / w, 148 * 8));
+    auto kern = g.np == 6 ? k_m2l_inv_rb<T, 6> : g.np == 4 ? k_m2l_inv_rb<T, 4> : k_m2l_inv_rb<T, 8>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    kern<<<gr, 32 * w, sm, st>>>(g, effval, work, nwork, tdncval);
+    return;
+  }
+  cudaFuncSetAttribute(k_m2l_inv_warp<T, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_m2l_inv_warp<T, 0><<<grid, 32 * wpc, smem, st>>>(g, effval, work, nwork, tdncval);
 }
 
 // ---------------------------------------------------------------------------
