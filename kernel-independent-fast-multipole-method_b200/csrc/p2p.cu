@@ -36,6 +36,56 @@ struct Red {
   T v[P2P_THREADS * TDMAX];
 };
 
+// Packed source tile: p[j] = (x, y, z, first density component); further
+// density components in f (SD-1 per point) and normals in n (double layer).
+// A single-dof single-layer interaction then reads one 16-byte (FP32) word.
+template <typename T>
+struct P4 {
+  T x, y, z, w;
+};
+
+template <typename T>
+struct PTile {
+  P4<T> p[TILE];
+  T f[TILE * 3];
+  T n[TILE * 3];
+};
+
+template <typename T, int KT>
+__device__ __forceinline__ void accumulate_ptile(const PTile<T>& t, int cnt, int j0, int jstep, T px, T py, T pz,
+                                                 T* acc, const KConst<T>& kc) {
+  constexpr int SD = KTraits<KT>::SD;
+  constexpr bool DL = KTraits<KT>::DL;
+#pragma unroll 4
+  for (int j = j0; j < cnt; j += jstep) {
+    const P4<T> s = t.p[j];
+    T f[SD];
+    f[0] = s.w;
+#pragma unroll
+    for (int k = 1; k < SD; k++) f[k] = t.f[j * (SD - 1) + k - 1];
+    T nrm[3];
+    if constexpr (DL) {
+      nrm[0] = t.n[3 * j];
+      nrm[1] = t.n[3 * j + 1];
+      nrm[2] = t.n[3 * j + 2];
+    }
+    keval<KT, T>(px - s.x, py - s.y, pz - s.z, nrm, f, acc, kc);
+  }
+}
+
+// writes point k of the tile
+template <typename T, int SD, bool DL>
+__device__ __forceinline__ void put_point(PTile<T>& t, int k, T x, T y, T z, const T* f, const T* nrm) {
+  t.p[k] = P4<T>{x, y, z, f[0]};
+#pragma unroll
+  for (int s = 1; s < SD; s++) t.f[k * (SD - 1) + s - 1] = f[s];
+  if constexpr (DL) {
+    t.n[3 * k] = nrm[0];
+    t.n[3 * k + 1] = nrm[1];
+    t.n[3 * k + 2] = nrm[2];
+  }
+}
+
 __device__ __forceinline__ int group_size(int nt) {
   int g = ((nt + 31) / 32) * 32;
   return g > P2P_THREADS ? P2P_THREADS : (g < 32 ? 32 : g);
@@ -113,37 +163,73 @@ __device__ __forceinline__ void reduce_and_store(Red<T, 4>& red, const T* acc, i
 }
 
 // ---------------------------------------------------------------------------
+// Each thread owns up to S2M_R upward check points (tid, tid + 128, ...), so a
+// staged source feeds all of them; the leaf's sources are staged once per tile.
+constexpr int S2M_R = 4;  // |UC| <= 488 (np = 8) <= 4 x 128
+
 template <typename T, int KT>
 __global__ void __launch_bounds__(P2P_THREADS) k_s2m(P2PArgs<T> a, const int* work, int nwork, int rhs) {
   constexpr int SD = KTraits<KT>::SD, TD = KTraits<KT>::TD;
   constexpr bool DL = KTraits<KT>::DL;
-  __shared__ Tile<T, 4> tile;
-  __shared__ Red<T, 4> red;
-  int g = work[blockIdx.x];
-  T rad = (T)a.radius[g];
-  int nt = a.nuc;
-  int G = group_size(nt), nsplit = P2P_THREADS / G;
-  int slot = threadIdx.x % G, sg = threadIdx.x / G;
-  int sb = a.sbeg[g], sc = a.scnt[g];
+  __shared__ PTile<T> tile;
+  const int g = work[blockIdx.x];
+  const T rad = (T)a.radius[g];
+  const int nt = a.nuc;
+  const int sb = a.sbeg[g], sc = a.scnt[g];
+  T px[S2M_R], py[S2M_R], pz[S2M_R], acc[S2M_R][4];
+#pragma unroll
+  for (int r = 0; r < S2M_R; r++) {
+    const int ti = threadIdx.x + r * P2P_THREADS;
+    px[r] = py[r] = pz[r] = T(0);
+    if (ti < nt) {
+      px[r] = a.uc_unit[3 * ti] * rad;
+      py[r] = a.uc_unit[3 * ti + 1] * rad;
+      pz[r] = a.uc_unit[3 * ti + 2] * rad;
+    }
+#pragma unroll
+    for (int d = 0; d < 4; d++) acc[r][d] = T(0);
+  }
+  const T* den = a.sden + (size_t)rhs * a.ns * SD;
+  for (int c0 = 0; c0 < sc; c0 += TILE) {
+    const int cnt = min(TILE, sc - c0);
+    __syncthreads();
+    for (int j = threadIdx.x; j < cnt; j += blockDim.x) {
+      const int p = sb + c0 + j;
+      T f[SD], nrm[3] = {T(0), T(0), T(0)};
+#pragma unroll
+      for (int s = 0; s < SD; s++) f[s] = den[(size_t)p * SD + s];
+      if constexpr (DL) {
+        nrm[0] = a.snx[p];
+        nrm[1] = a.sny[p];
+        nrm[2] = a.snz[p];
+      }
+      put_point<T, SD, DL>(tile, j, a.sx[p], a.sy[p], a.sz[p], f, nrm);
+    }
+    __syncthreads();
+    for (int j = 0; j < cnt; j++) {  // one staged source, every check point of this thread
+      const P4<T> sp = tile.p[j];
+      T f[SD];
+      f[0] = sp.w;
+#pragma unroll
+      for (int k = 1; k < SD; k++) f[k] = tile.f[j * (SD - 1) + k - 1];
+      T nrm[3];
+      if constexpr (DL) {
+        nrm[0] = tile.n[3 * j];
+        nrm[1] = tile.n[3 * j + 1];
+        nrm[2] = tile.n[3 * j + 2];
+      }
+#pragma unroll
+      for (int r = 0; r < S2M_R; r++)
+        if (threadIdx.x + r * P2P_THREADS < nt) keval<KT, T>(px[r] - sp.x, py[r] - sp.y, pz[r] - sp.z, nrm, f, acc[r], a.ku);
+    }
+  }
   T* outbase = a.supcval + (size_t)g * a.nuc * TD;
-  for (int tb = 0; tb < nt; tb += G) {
-    int ti = tb + slot;
-    bool valid = ti < nt && sg < nsplit;
-    T px = 0, py = 0, pz = 0;
-    if (valid) {
-      px = a.uc_unit[3 * ti] * rad;
-      py = a.uc_unit[3 * ti + 1] * rad;
-      pz = a.uc_unit[3 * ti + 2] * rad;
-    }
-    T acc[4] = {0, 0, 0, 0};
-    for (int c0 = 0; c0 < sc; c0 += TILE) {
-      int cnt = min(TILE, sc - c0);
-      __syncthreads();
-      stage_points<T, SD, DL>(tile, a, sb + c0, cnt, T(0), T(0), T(0), rhs);
-      __syncthreads();
-      if (valid) accumulate_tile<T, KT>(tile, cnt, sg, nsplit, px, py, pz, acc, a.ku);
-    }
-    reduce_and_store<T, TD>(red, acc, G, nsplit, ti < nt, outbase + (size_t)ti * TD, false);
+#pragma unroll
+  for (int r = 0; r < S2M_R; r++) {
+    const int ti = threadIdx.x + r * P2P_THREADS;
+    if (ti < nt)
+#pragma unroll
+      for (int d = 0; d < TD; d++) outbase[(size_t)ti * TD + d] = acc[r][d];
   }
 }
 
@@ -223,7 +309,7 @@ __global__ void __launch_bounds__(P2P_THREADS) k_leaf(P2PArgs<T> a, const int* w
   constexpr bool DL = KTraits<KT>::DL;
   constexpr int MM = KTraits<KT>::MM;
   constexpr int SDM = KTraits<MM>::SD;
-  __shared__ Tile<T, 4> tile;
+  __shared__ PTile<T> tile;
   __shared__ Red<T, 4> red;
   __shared__ Segs<T> seg;
   const int w = blockIdx.x;
@@ -237,8 +323,10 @@ __global__ void __launch_bounds__(P2P_THREADS) k_leaf(P2PArgs<T> a, const int* w
   const int slot = threadIdx.x % G, sg = threadIdx.x / G;
   const bool l2t = a.depth[g] >= 2;
   T* outbase = a.tval + (size_t)rhs * a.nt * TD;
+  const T* den = a.sden + (size_t)rhs * a.ns * SD;
   const int64_t nb = nptr[w], ne = nptr[w + 1];
   const int64_t mb = mptr[w], me = mptr[w + 1];
+  const int nsurf = a.nsurf;
   const int nsurf_segs = (int)(me - mb) + (l2t ? 1 : 0);
   for (int tb = 0; tb < nt; tb += G) {
     const int ti = tb + slot;
@@ -271,23 +359,23 @@ __global__ void __launch_bounds__(P2P_THREADS) k_leaf(P2PArgs<T> a, const int* w
       const int total = seg.pre[nseg];
       for (int k0 = 0; k0 < total; k0 += TILE) {
         const int cnt = min(TILE, total - k0);
+        // one thread per staged point; its source leaf by bisection of the prefix sums
         for (int j = threadIdx.x; j < cnt; j += blockDim.x) {
-          int k = k0 + j;
-          int e = find_seg(seg.pre, nseg, k);
-          int p = seg.beg[e] + (k - seg.pre[e]);
-          tile.x[j] = a.sx[p] + seg.shx[e];
-          tile.y[j] = a.sy[p] + seg.shy[e];
-          tile.z[j] = a.sz[p] + seg.shz[e];
-          if constexpr (DL) {
-            tile.nx[j] = a.snx[p];
-            tile.ny[j] = a.sny[p];
-            tile.nz[j] = a.snz[p];
-          }
+          const int k = k0 + j;
+          const int e = find_seg(seg.pre, nseg, k);
+          const int p = seg.beg[e] + (k - seg.pre[e]);
+          T f[SD], nrm[3] = {T(0), T(0), T(0)};
 #pragma unroll
-          for (int s = 0; s < SD; s++) tile.f[j * SD + s] = a.sden[(size_t)rhs * a.ns * SD + (size_t)p * SD + s];
+          for (int s = 0; s < SD; s++) f[s] = den[(size_t)p * SD + s];
+          if constexpr (DL) {
+            nrm[0] = a.snx[p];
+            nrm[1] = a.sny[p];
+            nrm[2] = a.snz[p];
+          }
+          put_point<T, SD, DL>(tile, j, a.sx[p] + seg.shx[e], a.sy[p] + seg.shy[e], a.sz[p] + seg.shz[e], f, nrm);
         }
         __syncthreads();
-        if (valid) accumulate_tile<T, KT>(tile, cnt, sg, nsplit, px, py, pz, acc, a.ku);
+        if (valid) accumulate_ptile<T, KT>(tile, cnt, sg, nsplit, px, py, pz, acc, a.ku);
         __syncthreads();
       }
     }
@@ -305,31 +393,32 @@ __global__ void __launch_bounds__(P2P_THREADS) k_leaf(P2PArgs<T> a, const int* w
           seg.shz[threadIdx.x] = (T)(a.center[3 * s + 2] - cz);
           seg.rad[threadIdx.x] = (T)a.radius[s];
           seg.unit[threadIdx.x] = a.ue_unit;
-          seg.den[threadIdx.x] = a.supeden + (size_t)s * a.nsurf * SDM;
+          seg.den[threadIdx.x] = a.supeden + (size_t)s * nsurf * SDM;
         } else {
           seg.shx[threadIdx.x] = seg.shy[threadIdx.x] = seg.shz[threadIdx.x] = T(0);
           seg.rad[threadIdx.x] = rad;
           seg.unit[threadIdx.x] = a.de_unit;
-          seg.den[threadIdx.x] = a.tdneden + (size_t)g * a.nsurf * SDM;
+          seg.den[threadIdx.x] = a.tdneden + (size_t)g * nsurf * SDM;
         }
       }
       __syncthreads();
-      const int total = nseg * a.nsurf;
+      const int total = nseg * nsurf;
       for (int k0 = 0; k0 < total; k0 += TILE) {
         const int cnt = min(TILE, total - k0);
         for (int j = threadIdx.x; j < cnt; j += blockDim.x) {
-          int k = k0 + j;
-          int e = k / a.nsurf, m = k - e * a.nsurf;
+          const int k = k0 + j;
+          const int e = k / nsurf, m = k - e * nsurf;
           const T* u = seg.unit[e];
-          T r = seg.rad[e];
-          tile.x[j] = u[3 * m] * r + seg.shx[e];
-          tile.y[j] = u[3 * m + 1] * r + seg.shy[e];
-          tile.z[j] = u[3 * m + 2] * r + seg.shz[e];
+          const T* sd = seg.den[e];
+          const T r = seg.rad[e];
+          T f[SDM];
 #pragma unroll
-          for (int s = 0; s < SDM; s++) tile.f[j * SDM + s] = seg.den[e][(size_t)m * SDM + s];
+          for (int s = 0; s < SDM; s++) f[s] = sd[(size_t)m * SDM + s];
+          put_point<T, SDM, false>(tile, j, u[3 * m] * r + seg.shx[e], u[3 * m + 1] * r + seg.shy[e],
+                                   u[3 * m + 2] * r + seg.shz[e], f, nullptr);
         }
         __syncthreads();
-        if (valid) accumulate_tile<T, MM>(tile, cnt, sg, nsplit, px, py, pz, acc, a.km);
+        if (valid) accumulate_ptile<T, MM>(tile, cnt, sg, nsplit, px, py, pz, acc, a.km);
         __syncthreads();
       }
     }
