@@ -524,7 +524,8 @@ struct Impl : ImplBase {
     s.lvl_base = E.rootlvl;
     if constexpr (sizeof(T) == 4) {
       if (A.tc.hi && ldb % 4 == 0 && ldc % 4 == 0) {
-        nlaunch += launch_node_gemm_tc(A.tc, B, ldb, bidx, C, ldc, cidx, ncol, acc, s, d_status, st);
+        nlaunch += launch_node_gemm_tc(A.tc, B, ldb, bidx, C, ldc, cidx, ncol, acc, s, gemm_ws, gemm_ws_len, num_sms,
+                                       d_status, st);
         return;
       }
     }

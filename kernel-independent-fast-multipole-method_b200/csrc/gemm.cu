@@ -154,6 +154,14 @@ int launch_node_gemm(int M, int K, const T* A, const T* B, int64_t ldb, const in
   return ks > 1 ? 2 : 1;
 }
 
+void launch_node_gemm_reduce_f(int M, int ncol, int nslice, const double* partial, float* C, int64_t ldc,
+                               const int* cidx, bool accumulate, const GemmScale& sc, int num_sms, cudaStream_t st) {
+  const size_t n = (size_t)ncol * M;
+  if (!n) return;
+  int g = (int)std::min<size_t>((n + 255) / 256, (size_t)num_sms * 8);
+  k_node_gemm_reduce<float><<<g, 256, 0, st>>>(M, ncol, nslice, partial, C, ldc, cidx, accumulate ? 1 : 0, sc);
+}
+
 template int launch_node_gemm<double>(int, int, const double*, const double*, int64_t, const int*, double*,
                                                int64_t, const int*, int, bool, const GemmScale&, double*, size_t, int,
                                                cudaStream_t);

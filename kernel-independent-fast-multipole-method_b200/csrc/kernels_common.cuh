@@ -35,7 +35,19 @@ struct KConst {
 };
 
 #ifdef __CUDACC__
-__device__ __forceinline__ float rsqrt_t(float x) { return rsqrtf(x); }
+// explicit fused multiply-add a*b + c: `u += p*q + r*s` written with two of
+// these is two instructions, where the expression form leaves an unfused
+// product and a separate add
+__device__ __forceinline__ float fmt(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fmt(double a, double b, double c) { return __fma_rn(a, b, c); }
+
+// FP32: the hardware approximation with denormal inputs flushed (every caller
+// has r^2 >= 1e-16), which drops the denormal rescaling steps of rsqrtf
+__device__ __forceinline__ float rsqrt_t(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
 __device__ __forceinline__ double rsqrt_t(double x) { return rsqrt(x); }
 
 template <int KT, typename T>
@@ -51,15 +63,16 @@ __device__ __forceinline__ void keval(T x, T y, T z, const T* nrm, const T* f, T
     T ri3 = ri * ri * ri;
     T xf = x * f[0] + y * f[1] + z * f[2];
     T g1 = k.c0 * ri, g3 = k.c0 * ri3 * xf, a3 = k.c1 * ri3 * f[3];
-    u[0] += g1 * f[0] + (g3 + a3) * x;
-    u[1] += g1 * f[1] + (g3 + a3) * y;
-    u[2] += g1 * f[2] + (g3 + a3) * z;
+    const T g = g3 + a3;
+    u[0] = fmt(g, x, fmt(g1, f[0], u[0]));
+    u[1] = fmt(g, y, fmt(g1, f[1], u[1]));
+    u[2] = fmt(g, z, fmt(g1, f[2], u[2]));
   } else if constexpr (KT == 311) {  // (delta/r + r r^T / r^3) / (8 pi mu)
     T xf = x * f[0] + y * f[1] + z * f[2];
     T g1 = k.c0 * ri, g3 = k.c0 * ri * ri * ri * xf;
-    u[0] += g1 * f[0] + g3 * x;
-    u[1] += g1 * f[1] + g3 * y;
-    u[2] += g1 * f[2] + g3 * z;
+    u[0] = fmt(g3, x, fmt(g1, f[0], u[0]));
+    u[1] = fmt(g3, y, fmt(g1, f[1], u[1]));
+    u[2] = fmt(g3, z, fmt(g1, f[2], u[2]));
   } else if constexpr (KT == 312) {  // (r.f) / (4 pi r^3)
     T xf = x * f[0] + y * f[1] + z * f[2];
     u[0] += k.c0 * ri * ri * ri * xf;
@@ -80,9 +93,9 @@ __device__ __forceinline__ void keval(T x, T y, T z, const T* nrm, const T* f, T
   } else if constexpr (KT == 511) {  // Kelvin solution
     T xf = x * f[0] + y * f[1] + z * f[2];
     T g1 = k.c0 * ri, g3 = k.c1 * ri * ri * ri * xf;
-    u[0] += g1 * f[0] + g3 * x;
-    u[1] += g1 * f[1] + g3 * y;
-    u[2] += g1 * f[2] + g3 * z;
+    u[0] = fmt(g3, x, fmt(g1, f[0], u[0]));
+    u[1] = fmt(g3, y, fmt(g1, f[1], u[1]));
+    u[2] = fmt(g3, z, fmt(g1, f[2], u[2]));
   } else if constexpr (KT == 521) {  // Navier double layer
     T xf = x * f[0] + y * f[1] + z * f[2];
     T nf = nrm[0] * f[0] + nrm[1] * f[1] + nrm[2] * f[2];
@@ -90,9 +103,9 @@ __device__ __forceinline__ void keval(T x, T y, T z, const T* nrm, const T* f, T
     T ri2 = ri * ri, ri3 = ri2 * ri;
     T A = k.c0 * ri3, B = k.c1 * ri3, C = k.c2 * ri3 * ri2;
     T s0 = A * rn, s1 = A * xf, s2 = B * nf + C * rn * xf;
-    u[0] += s0 * f[0] + s1 * nrm[0] + s2 * x;
-    u[1] += s0 * f[1] + s1 * nrm[1] + s2 * y;
-    u[2] += s0 * f[2] + s1 * nrm[2] + s2 * z;
+    u[0] = fmt(s2, x, fmt(s1, nrm[0], fmt(s0, f[0], u[0])));
+    u[1] = fmt(s2, y, fmt(s1, nrm[1], fmt(s0, f[1], u[1])));
+    u[2] = fmt(s2, z, fmt(s1, nrm[2], fmt(s0, f[2], u[2])));
   }
 }
 

@@ -79,16 +79,21 @@ int launch_node_gemm(int M, int K, const T* A, const T* B, int64_t ldb, const in
 // about 2^-21 relative per product, the FP32 rounding class.  The operator is
 // pre-split on the host: hi/lo are Np x Kp row-major (Np = M rounded up to 16,
 // Kp = K rounded up to 32, zero padded).  Requires K, ldb, ldc multiples of 4
-// and 16-byte aligned B and C.  A bounded wait that times out sets bit 1 of
-// *status.  Returns the number of launches.
+// and 16-byte aligned B and C.  Launches with fewer tiles than SMs split K
+// over CTAs into ws (FP64, ws_len doubles) and reduce it deterministically.
+// A bounded wait that times out sets bit 1 of *status.  Returns the number
+// of launches.
 struct TcOperator {
   const float* hi = nullptr;
   const float* lo = nullptr;
   int M = 0, K = 0, Np = 0, Kp = 0;
 };
 int launch_node_gemm_tc(const TcOperator& A, const float* B, int64_t ldb, const int* bidx, float* C, int64_t ldc,
-                        const int* cidx, int ncol, bool accumulate, const GemmScale& sc, int* status,
-                        cudaStream_t st);
+                        const int* cidx, int ncol, bool accumulate, const GemmScale& sc, double* ws, size_t ws_len,
+                        int num_sms, int* status, cudaStream_t st);
+// C[cidx[j]] (=|+=) scaled sum over nslice of partial[z][j][0..M) (gemm.cu)
+void launch_node_gemm_reduce_f(int M, int ncol, int nslice, const double* partial, float* C, int64_t ldc,
+                               const int* cidx, bool accumulate, const GemmScale& sc, int num_sms, cudaStream_t st);
 // host-side split of a row-major M x K operator into the padded hi/lo pair
 void split_tf32(int M, int K, const double* A, std::vector<float>* hi, std::vector<float>* lo, int* Np, int* Kp);
 

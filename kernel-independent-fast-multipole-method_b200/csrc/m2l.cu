@@ -121,8 +121,8 @@ __global__ void __launch_bounds__(256) k_m2l_fwd_warp(M2LGeom g, const T* __rest
         for (int j = 0; j < np; j++) {
           Cpx<T> a = A[(k * np + j) * nh + kx];
           Cpx<T> t = W2[j * n + ky];
-          re += a.re * t.re - a.im * t.im;
-          im += a.re * t.im + a.im * t.re;
+          re = fmt(-a.im, t.im, fmt(a.re, t.re, re));
+          im = fmt(a.im, t.re, fmt(a.re, t.im, im));
         }
         Bm[e].re = re;
         Bm[e].im = im;
@@ -138,8 +138,8 @@ __global__ void __launch_bounds__(256) k_m2l_fwd_warp(M2LGeom g, const T* __rest
         for (int k = 0; k < np; k++) {
           Cpx<T> b = Bm[k * n * nh + kxy];
           Cpx<T> t = W2[k * n + kz];
-          r.re += b.re * t.re - b.im * t.im;
-          r.im += b.re * t.im + b.im * t.re;
+          r.re = fmt(-b.im, t.im, fmt(b.re, t.re, r.re));
+          r.im = fmt(b.im, t.re, fmt(b.re, t.im, r.im));
         }
         out[c] = r;
       }
@@ -185,8 +185,8 @@ __global__ void __launch_bounds__(256) k_m2l_inv_warp(M2LGeom g, const T* __rest
         for (int kz = 0; kz < n; kz++) {
           Cpx<T> y = Y[kz * n * nh + kxy];
           Cpx<T> c = W2[k * n + kz];
-          re += y.re * c.re + y.im * c.im;
-          im += y.im * c.re - y.re * c.im;
+          re = fmt(y.im, c.im, fmt(y.re, c.re, re));
+          im = fmt(-y.re, c.im, fmt(y.im, c.re, im));
         }
         Bm[e].re = re;
         Bm[e].im = im;
@@ -199,8 +199,8 @@ __global__ void __launch_bounds__(256) k_m2l_inv_warp(M2LGeom g, const T* __rest
         for (int ky = 0; ky < n; ky++) {
           Cpx<T> b = Bm[(k * n + ky) * nh + kx];
           Cpx<T> c = W2[j * n + ky];
-          re += b.re * c.re + b.im * c.im;
-          im += b.im * c.re - b.re * c.im;
+          re = fmt(b.im, c.im, fmt(b.re, c.re, re));
+          im = fmt(-b.re, c.im, fmt(b.im, c.re, im));
         }
         A[e].re = re;
         A[e].im = im;
@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(256) k_m2l_inv_warp(M2LGeom g, const T* __rest
 #pragma unroll
         for (int kx = 1; kx < nh - 1; kx++) {
           Cpx<T> c = W2[i * n + kx];
-          acc += a[kx].re * c.re + a[kx].im * c.im;
+          acc = fmt(a[kx].im, c.im, fmt(a[kx].re, c.re, acc));
         }
         dst[(size_t)m * g.td + t] += v + T(2) * acc;
       }
@@ -267,8 +267,8 @@ __global__ void __launch_bounds__(FFT_THREADS) k_m2l_had(M2LGeom g, const T* __r
           for (int s = 0; s < SD; s++) {
             T kr = K[(((size_t)d * SD + s) * nf + f) * 2];
             T ki = K[(((size_t)d * SD + s) * nf + f) * 2 + 1];
-            ar[d] += kr * xr[s] - ki * xi[s];
-            ai[d] += kr * xi[s] + ki * xr[s];
+            ar[d] = fmt(-ki, xi[s], fmt(kr, xr[s], ar[d]));
+            ai[d] = fmt(ki, xr[s], fmt(kr, xi[s], ai[d]));
           }
       }
     }
@@ -418,8 +418,8 @@ __global__ void __launch_bounds__(256) k_m2l_fwd_rb(M2LGeom g, const T* __restri
 #pragma unroll
           for (int j = 0; j < NP; j++) {
             const T c = twr<T, N>(j * ky), d = twi<T, N>(j * ky);
-            re += a[j].re * c - a[j].im * d;
-            im += a[j].re * d + a[j].im * c;
+            re = fmt(-a[j].im, d, fmt(a[j].re, c, re));
+            im = fmt(a[j].im, c, fmt(a[j].re, d, im));
           }
           Bm[(k * N + ky) * NH + kx] = Cpx<T>{re, im};
         }
@@ -440,8 +440,8 @@ __global__ void __launch_bounds__(256) k_m2l_fwd_rb(M2LGeom g, const T* __restri
 #pragma unroll
           for (int k = 0; k < NP; k++) {
             const T cr = twr<T, N>(k * kz), ci = twi<T, N>(k * kz);
-            re += b[k].re * cr - b[k].im * ci;
-            im += b[k].re * ci + b[k].im * cr;
+            re = fmt(-b[k].im, ci, fmt(b[k].re, cr, re));
+            im = fmt(b[k].im, cr, fmt(b[k].re, ci, im));
           }
           out[c] = Cpx<T>{re, im};
         }
@@ -493,8 +493,8 @@ __global__ void __launch_bounds__(256) k_m2l_inv_rb(M2LGeom g, const T* __restri
 #pragma unroll
           for (int kz = 0; kz < N; kz++) {
             const T cr = twr<T, N>(k * kz), ci = twi<T, N>(k * kz);
-            re += y[kz].re * cr + y[kz].im * ci;
-            im += y[kz].im * cr - y[kz].re * ci;
+            re = fmt(y[kz].im, ci, fmt(y[kz].re, cr, re));
+            im = fmt(-y[kz].re, ci, fmt(y[kz].im, cr, im));
           }
           Bm[(k * N + ky) * NH + kx] = Cpx<T>{re, im};
         }
@@ -512,8 +512,8 @@ __global__ void __launch_bounds__(256) k_m2l_inv_rb(M2LGeom g, const T* __restri
 #pragma unroll
           for (int ky = 0; ky < N; ky++) {
             const T cr = twr<T, N>(j * ky), ci = twi<T, N>(j * ky);
-            re += b[ky].re * cr + b[ky].im * ci;
-            im += b[ky].im * cr - b[ky].re * ci;
+            re = fmt(b[ky].im, ci, fmt(b[ky].re, cr, re));
+            im = fmt(-b[ky].re, ci, fmt(b[ky].im, cr, im));
           }
           A[(k * NP + j) * NH + kx] = Cpx<T>{re, im};
         }
@@ -533,7 +533,7 @@ __global__ void __launch_bounds__(256) k_m2l_inv_rb(M2LGeom g, const T* __restri
           T acc = 0;
 #pragma unroll
           for (int kx = 1; kx < NH - 1; kx++)
-            acc += a[kx].re * twr<T, N>(i * kx) + a[kx].im * twi<T, N>(i * kx);
+            acc = fmt(a[kx].im, twi<T, N>(i * kx), fmt(a[kx].re, twr<T, N>(i * kx), acc));
           const T v = a[0].re + ((i & 1) ? -a[NH - 1].re : a[NH - 1].re);
           dst[(size_t)m * g.td + t] += v + T(2) * acc;
         }
@@ -734,8 +734,8 @@ __device__ __forceinline__ void sweep_tile(const Cpx<T>* __restrict__ Ks, const 
           const Cpx<T> k = Kd[cij * 32];
 #pragma unroll
           for (int q = 0; q < QPT; q++) {
-            ar[q][i] += k.re * xr[q][j] - k.im * xi[q][j];
-            ai[q][i] += k.re * xi[q][j] + k.im * xr[q][j];
+            ar[q][i] = fmt(-k.im, xi[q][j], fmt(k.re, xr[q][j], ar[q][i]));
+            ai[q][i] = fmt(k.im, xr[q][j], fmt(k.re, xi[q][j], ai[q][i]));
           }
         }
       }

@@ -56,20 +56,35 @@ __device__ __forceinline__ void accumulate_ptile(const PTile<T>& t, int cnt, int
                                                  T* acc, const KConst<T>& kc) {
   constexpr int SD = KTraits<KT>::SD;
   constexpr bool DL = KTraits<KT>::DL;
+  const int rounds = j0 < cnt ? (cnt - j0 + jstep - 1) / jstep : 0;
+  if constexpr (KT == 111) {  // sum f / r, times 1/(4 pi) once
+    T s1 = T(0);
 #pragma unroll 4
-  for (int j = j0; j < cnt; j += jstep) {
-    const P4<T> s = t.p[j];
-    T f[SD];
-    f[0] = s.w;
-#pragma unroll
-    for (int k = 1; k < SD; k++) f[k] = t.f[j * (SD - 1) + k - 1];
-    T nrm[3];
-    if constexpr (DL) {
-      nrm[0] = t.n[3 * j];
-      nrm[1] = t.n[3 * j + 1];
-      nrm[2] = t.n[3 * j + 2];
+    for (int r = 0; r < rounds; r++) {
+      const P4<T> s = t.p[j0 + r * jstep];
+      const T x = px - s.x, y = py - s.y, z = pz - s.z;
+      const T r2 = x * x + y * y + z * z;
+      const T ri = (r2 >= T(1e-16)) ? rsqrt_t(r2) : T(0);
+      s1 += ri * s.w;
     }
-    keval<KT, T>(px - s.x, py - s.y, pz - s.z, nrm, f, acc, kc);
+    acc[0] += kc.c0 * s1;
+  } else {
+#pragma unroll 4
+    for (int r = 0; r < rounds; r++) {
+      const int j = j0 + r * jstep;
+      const P4<T> s = t.p[j];
+      T f[SD];
+      f[0] = s.w;
+#pragma unroll
+      for (int k = 1; k < SD; k++) f[k] = t.f[j * (SD - 1) + k - 1];
+      T nrm[3];
+      if constexpr (DL) {
+        nrm[0] = t.n[3 * j];
+        nrm[1] = t.n[3 * j + 1];
+        nrm[2] = t.n[3 * j + 2];
+      }
+      keval<KT, T>(px - s.x, py - s.y, pz - s.z, nrm, f, acc, kc);
+    }
   }
 }
 
