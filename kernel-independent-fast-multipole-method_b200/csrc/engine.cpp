@@ -193,16 +193,19 @@ struct Impl : ImplBase {
         kh[2 * i + 1] = (T)op.m2l[i].imag();
       }
       khat = upload(kh);
-      if (sd_m == 1 && td_m == 1 && m2l_sweep_supported(op.nfc)) {
-        const int nf = op.nfc, ftiles = (nf + 31) / 32;
-        std::vector<T> kt((size_t)ftiles * 343 * 32 * 2, T(0));
-        for (int ft = 0; ft < ftiles; ft++)
-          for (int o = 0; o < 343; o++)
-            for (int l = 0; l < 32 && ft * 32 + l < nf; l++) {
-              size_t dst = (((size_t)ft * 343 + o) * 32 + l) * 2;
-              kt[dst] = kh[((size_t)o * nf + ft * 32 + l) * 2];
-              kt[dst + 1] = kh[((size_t)o * nf + ft * 32 + l) * 2 + 1];
-            }
+      if (m2l_sweep_supported(op.nfc, sd_m, td_m)) {
+        // [td][sd][ftile][343][32]; the spectra are [343][td][sd][nf]
+        const int nf = op.nfc, ftiles = (nf + 31) / 32, tsd = td_m * sd_m;
+        std::vector<T> kt((size_t)tsd * ftiles * 343 * 32 * 2, T(0));
+        for (int ts = 0; ts < tsd; ts++)
+          for (int ft = 0; ft < ftiles; ft++)
+            for (int o = 0; o < 343; o++)
+              for (int l = 0; l < 32 && ft * 32 + l < nf; l++) {
+                const size_t dst = ((((size_t)ts * ftiles + ft) * 343 + o) * 32 + l) * 2;
+                const size_t src = (((size_t)o * tsd + ts) * nf + ft * 32 + l) * 2;
+                kt[dst] = kh[src];
+                kt[dst + 1] = kh[src + 1];
+              }
         ktiles = upload(kt);
       }
     }
@@ -573,13 +576,13 @@ struct Impl : ImplBase {
         launch_m2l_forward<T>(geom, supeden, fwd.work, fwd.n, d_depth, spectra, st);
         if (prof && r == 0) KCHECK(cudaEventRecord(ev[7], st));
         if (pairs_n > 0)
-          launch_m2l_hadamard_sweep<T>(op.nfc, ktiles, spectra, pairs_n, pairs_chd, pairs_coll, pairs_mask, effval,
-                                       tr.nnodes, d_status, num_sms, st);
+          launch_m2l_hadamard_sweep<T>(op.nfc, sd_m, td_m, ktiles, spectra, pairs_n, pairs_chd, pairs_coll,
+                                       pairs_mask, effval, tr.nnodes, d_status, num_sms, st);
         else
           launch_m2l_hadamard<T>(geom, khat, spectra, m2l.work, m2l.n, m2l.ptr, m2l.idx, d_path, effval, st);
         if (prof && r == 0) KCHECK(cudaEventRecord(ev[8], st));
         launch_m2l_inverse<T>(geom, effval, m2l.work, m2l.n, tdncval, st);
-        nlaunch += 3;
+        nlaunch += 2 + (pairs_n > 0 ? sd_m * td_m : 1);
       }
       if (prof && r == 0) KCHECK(cudaEventRecord(ev[2], st));
       // X list

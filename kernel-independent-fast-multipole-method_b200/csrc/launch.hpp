@@ -118,17 +118,18 @@ void launch_m2l_forward(const M2LGeom& g, const T* supeden, const int* nodes, in
 template <typename T>
 void launch_m2l_hadamard(const M2LGeom& g, const T* khat, const T* spectra, const int* work, int nwork,
                          const int64_t* vptr, const int* vidx, const int* path, T* effval, cudaStream_t st);
-// Parent-pair form for single-dof kernels: effval[child of Q] for the nq target
-// parents Q (first child qchd[q], colleague first children coll[q][26], the
-// all-zero block zero_node when absent, V-list children mask[q]).  ktiles:
-// operator spectra as [ceil(nf/32)][343][32] complex, zero-padded.  A mbarrier
-// wait that times out sets bit 0 of *status.  nf must satisfy
-// m2l_sweep_supported (np = 4, 6, 8).
-bool m2l_sweep_supported(int nf);
+// Parent-pair form: effval[child of Q] for the nq target parents Q (first
+// child qchd[q], colleague first children coll[q][26], the all-zero block
+// zero_node when absent, V-list children mask[q]).  ktiles: operator spectra
+// as [td][sd][ceil(nf/32)][343][32] complex, zero-padded; one pass per
+// (target dof, source dof).  A mbarrier wait that times out sets bit 0 of
+// *status.  Requires m2l_sweep_supported(nf, sd, td) (np = 4, 6, 8; dofs
+// 1->1, 4->3, 3->3).
+bool m2l_sweep_supported(int nf, int sd, int td);
 template <typename T>
-void launch_m2l_hadamard_sweep(int nf, const T* ktiles, const T* spectra, int nq, const int* qchd, const int* coll,
-                               const unsigned char* mask, T* effval, int zero_node, int* status, int num_sms,
-                               cudaStream_t st);
+void launch_m2l_hadamard_sweep(int nf, int sd, int td, const T* ktiles, const T* spectra, int nq, const int* qchd,
+                               const int* coll, const unsigned char* mask, T* effval, int zero_node, int* status,
+                               int num_sms, cudaStream_t st);
 // tdncval[node] += extract(inverse(effval[node]))
 template <typename T>
 void launch_m2l_inverse(const M2LGeom& g, const T* effval, const int* work, int nwork, T* tdncval,

@@ -663,11 +663,14 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned parity)
 
 // The work of one frequency tile for one warp: claim QPT target parents at a
 // time from *claim until the CTA's slice [.., qend) is exhausted.
-template <typename T, int NF, int QPT>
+// SD / TD: dofs per node of the source / target spectra; this pass reads
+// source component sc and adds into target component tc (first sc writes).
+template <typename T, int NF, int QPT, int SD, int TD>
 __device__ __forceinline__ void sweep_tile(const Cpx<T>* __restrict__ Ks, const Cpx<T>* __restrict__ spectra,
                                            int* claim, int qend, int f, const int* __restrict__ qchd,
                                            const int* __restrict__ coll, const unsigned char* __restrict__ mask,
-                                           Cpx<T>* __restrict__ effval, int zero_node) {
+                                           Cpx<T>* __restrict__ effval, int zero_node, int sc, int tc, bool acc) {
+  constexpr int XS = SD * NF;  // source child stride
   const int lane = threadIdx.x & 31;
   const int fl = min(f, NF - 1);  // lanes past NF load a valid spectrum and store nothing
   while (true) {
@@ -688,10 +691,10 @@ __device__ __forceinline__ void sweep_tile(const Cpx<T>* __restrict__ Ks, const 
 #pragma unroll
     for (int q = 0; q < QPT; q++) {
       nb[q] = (q0 + q < qend) ? cq[q][0] : zero_node;
-      const Cpx<T>* X = spectra + (size_t)nb[q] * NF + fl;
+      const Cpx<T>* X = spectra + ((size_t)nb[q] * SD + sc) * NF + fl;
 #pragma unroll
       for (int j = 0; j < 8; j++) {
-        Cpx<T> x = X[j * NF];
+        Cpx<T> x = X[j * XS];
         nxr[q][j] = x.re;
         nxi[q][j] = x.im;
       }
@@ -712,10 +715,10 @@ __device__ __forceinline__ void sweep_tile(const Cpx<T>* __restrict__ Ks, const 
 #pragma unroll
         for (int q = 0; q < QPT; q++) {
           nb[q] = (q0 + q < qend) ? cq[q][dir + 1] : zero_node;
-          const Cpx<T>* X = spectra + (size_t)nb[q] * NF + fl;
+          const Cpx<T>* X = spectra + ((size_t)nb[q] * SD + sc) * NF + fl;
 #pragma unroll
           for (int j = 0; j < 8; j++) {
-            Cpx<T> x = X[j * NF];
+            Cpx<T> x = X[j * XS];
             nxr[q][j] = x.re;
             nxi[q][j] = x.im;
           }
@@ -749,10 +752,16 @@ __device__ __forceinline__ void sweep_tile(const Cpx<T>* __restrict__ Ks, const 
 #pragma unroll
         for (int i = 0; i < 8; i++) {
           if (!((m >> i) & 1)) continue;
+          Cpx<T>* py = effval + ((size_t)(c0 + i) * TD + tc) * NF + f;
           Cpx<T> y;
           y.re = ar[q][i];
           y.im = ai[q][i];
-          effval[(size_t)(c0 + i) * NF + f] = y;
+          if (acc) {
+            const Cpx<T> o = *py;
+            y.re += o.re;
+            y.im += o.im;
+          }
+          *py = y;
         }
       }
     }
@@ -766,13 +775,13 @@ __device__ __forceinline__ void sweep_tile(const Cpx<T>* __restrict__ Ks, const 
 // mbarrier arrive releases the reset to the warps that wait on that buffer.
 // NBUF = 1 (FP64, one 176 KB tile): the tile is reloaded between two CTA
 // barriers.
-template <typename T, int NF, int QPT, int NTHR, int NBUF>
+template <typename T, int NF, int QPT, int NTHR, int NBUF, int SD, int TD>
 __global__ void __launch_bounds__(NTHR) k_m2l_had_sweep(const Cpx<T>* __restrict__ ktiles,
                                                        const Cpx<T>* __restrict__ spectra, int nq,
                                                        const int* __restrict__ qchd, const int* __restrict__ coll,
                                                        const unsigned char* __restrict__ mask,
-                                                       Cpx<T>* __restrict__ effval, int zero_node,
-                                                       int* __restrict__ status) {
+                                                       Cpx<T>* __restrict__ effval, int zero_node, int sc, int tc,
+                                                       int acc, int* __restrict__ status) {
   constexpr int TILE = 343 * 32;
   constexpr unsigned TILE_BYTES = TILE * sizeof(Cpx<T>);
   constexpr int FTILES = (NF + 31) / 32;
@@ -806,8 +815,8 @@ __global__ void __launch_bounds__(NTHR) k_m2l_had_sweep(const Cpx<T>* __restrict
         if (lane == 0) atomicOr(status, 1);
         return;
       }
-      sweep_tile<T, NF, QPT>(Kbuf + (size_t)b * TILE, spectra, &claim[b], qend, ft * 32 + lane, qchd, coll, mask,
-                             effval, zero_node);
+      sweep_tile<T, NF, QPT, SD, TD>(Kbuf + (size_t)b * TILE, spectra, &claim[b], qend, ft * 32 + lane, qchd, coll,
+                                     mask, effval, zero_node, sc, tc, acc != 0);
       if (lane == 0) {
         if (atomicAdd(&done_cnt[b], 1) == NW - 1) {  // the last warp out of tile ft
           done_cnt[b] = 0;
@@ -831,13 +840,14 @@ __global__ void __launch_bounds__(NTHR) k_m2l_had_sweep(const Cpx<T>* __restrict
         if (threadIdx.x == 0) atomicOr(status, 1);
         return;
       }
-      sweep_tile<T, NF, QPT>(Kbuf, spectra, &claim[0], qend, ft * 32 + lane, qchd, coll, mask, effval, zero_node);
+      sweep_tile<T, NF, QPT, SD, TD>(Kbuf, spectra, &claim[0], qend, ft * 32 + lane, qchd, coll, mask, effval,
+                                     zero_node, sc, tc, acc != 0);
       __syncthreads();
     }
   }
 }
 
-template <typename T, int NF>
+template <typename T, int NF, int SD, int TD>
 void sweep_launch(const T* ktiles, const T* spectra, int nq, const int* qchd, const int* coll,
                   const unsigned char* mask, T* effval, int zero_node, int* status, int num_sms, cudaStream_t st) {
   constexpr int QPT = 2;
@@ -846,32 +856,53 @@ void sweep_launch(const T* ktiles, const T* spectra, int nq, const int* qchd, co
   constexpr int NTHR = sizeof(T) == 4 ? 512 : 256;
   constexpr int NBUF = sizeof(T) == 4 ? 2 : 1;
   const size_t smem = (size_t)NBUF * 343 * 32 * sizeof(Cpx<T>);
-  auto kern = k_m2l_had_sweep<T, NF, QPT, NTHR, NBUF>;
+  auto kern = k_m2l_had_sweep<T, NF, QPT, NTHR, NBUF, SD, TD>;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  int grid = std::max(1, std::min(num_sms, (nq + QPT - 1) / QPT));
-  kern<<<grid, NTHR, smem, st>>>(reinterpret_cast<const Cpx<T>*>(ktiles), reinterpret_cast<const Cpx<T>*>(spectra),
-                                 nq, qchd, coll, mask, reinterpret_cast<Cpx<T>*>(effval), zero_node, status);
+  // at least 32 target parents per CTA: each CTA streams every operator tile
+  // (28 x 88 KB at np = 6), which a handful of parents would not amortise
+  const int grid = std::max(1, std::min(num_sms, nq / 32));
+  const size_t tiles = (size_t)((NF + 31) / 32) * 343 * 32;  // Cpx per (t, s) operator table
+  // one pass per (target dof, source dof); the first source dof writes
+  for (int t = 0; t < TD; t++)
+    for (int s = 0; s < SD; s++)
+      kern<<<grid, NTHR, smem, st>>>(reinterpret_cast<const Cpx<T>*>(ktiles) + (size_t)(t * SD + s) * tiles,
+                                     reinterpret_cast<const Cpx<T>*>(spectra), nq, qchd, coll, mask,
+                                     reinterpret_cast<Cpx<T>*>(effval), zero_node, s, t, s > 0 ? 1 : 0, status);
+}
+
+template <typename T, int NF>
+void sweep_dofs(int sd, int td, const T* ktiles, const T* spectra, int nq, const int* qchd, const int* coll,
+                const unsigned char* mask, T* effval, int zero_node, int* status, int num_sms, cudaStream_t st) {
+  if (sd == 1 && td == 1)
+    sweep_launch<T, NF, 1, 1>(ktiles, spectra, nq, qchd, coll, mask, effval, zero_node, status, num_sms, st);
+  else if (sd == 4 && td == 3)
+    sweep_launch<T, NF, 4, 3>(ktiles, spectra, nq, qchd, coll, mask, effval, zero_node, status, num_sms, st);
+  else if (sd == 3 && td == 3)
+    sweep_launch<T, NF, 3, 3>(ktiles, spectra, nq, qchd, coll, mask, effval, zero_node, status, num_sms, st);
 }
 
 }  // namespace
 
-bool m2l_sweep_supported(int nf) { return nf == 260 || nf == 868 || nf == 2052; }
+bool m2l_sweep_supported(int nf, int sd, int td) {
+  return (nf == 260 || nf == 868 || nf == 2052) &&
+         ((sd == 1 && td == 1) || (sd == 4 && td == 3) || (sd == 3 && td == 3));
+}
 
 template <typename T>
-void launch_m2l_hadamard_sweep(int nf, const T* ktiles, const T* spectra, int nq, const int* qchd, const int* coll,
-                               const unsigned char* mask, T* effval, int zero_node, int* status, int num_sms,
-                               cudaStream_t st) {
+void launch_m2l_hadamard_sweep(int nf, int sd, int td, const T* ktiles, const T* spectra, int nq, const int* qchd,
+                               const int* coll, const unsigned char* mask, T* effval, int zero_node, int* status,
+                               int num_sms, cudaStream_t st) {
   if (nq <= 0) return;
   if (nf == 868)
-    sweep_launch<T, 868>(ktiles, spectra, nq, qchd, coll, mask, effval, zero_node, status, num_sms, st);
+    sweep_dofs<T, 868>(sd, td, ktiles, spectra, nq, qchd, coll, mask, effval, zero_node, status, num_sms, st);
   else if (nf == 260)
-    sweep_launch<T, 260>(ktiles, spectra, nq, qchd, coll, mask, effval, zero_node, status, num_sms, st);
+    sweep_dofs<T, 260>(sd, td, ktiles, spectra, nq, qchd, coll, mask, effval, zero_node, status, num_sms, st);
   else if (nf == 2052)
-    sweep_launch<T, 2052>(ktiles, spectra, nq, qchd, coll, mask, effval, zero_node, status, num_sms, st);
+    sweep_dofs<T, 2052>(sd, td, ktiles, spectra, nq, qchd, coll, mask, effval, zero_node, status, num_sms, st);
 }
 
 #define KIFMM_INST(T)                                                                                             \
-  template void launch_m2l_hadamard_sweep<T>(int, const T*, const T*, int, const int*, const int*,               \
+  template void launch_m2l_hadamard_sweep<T>(int, int, int, const T*, const T*, int, const int*, const int*,     \
                                              const unsigned char*, T*, int, int*, int, cudaStream_t);              \
   template void launch_m2l_forward<T>(const M2LGeom&, const T*, const int*, int, const int*, T*, cudaStream_t);  \
   template void launch_m2l_hadamard<T>(const M2LGeom&, const T*, const T*, const int*, int, const int64_t*,     \
