@@ -7,8 +7,8 @@ seeded synthetic data (no dataset is involved).  A step is one FMM3d::eval
 (device-resident densities in, device-resident potentials out) of that whole
 point cloud; setup (tree, lists, operators) is done once, outside timing.
 
-  value      Mpoints/s of the mixed-precision engine (FP32 bulk, FP64
-             pseudo-inverse products), all ranks together
+  value      Mpoints/s of the mixed-precision engine (FP32 bulk, surface
+             contractions in split TF32 on the tensor cores), all ranks together
   fp64       the plain FP64 GPU engine on the same workload
   batched    64 independent instances (48 Laplace + 16 Stokes single-layer,
              np=6, log-uniform sizes in [1e4, 5e5], sphere / cube / Plummer
@@ -417,12 +417,19 @@ def engine_arm(args):
     had_ms = phases.get("m2l_hadamard") or phases["vlist"]
     achieved = alg_bytes / (had_ms / 1e3) / 1e9
     had_flops = wc["v_pairs"] * nf * 8
+    # DRAM traffic per launch: 14,220 B per spectrum node, read + write, from the
+    # ncu capture of this kernel on the 1M-point case (profiles/hadamard_sweep_*),
+    # scaled by the spectra of this workload
+    traffic = 14220.0 * wc["fwd_spectra"]
+    sm_mhz = clk.get("sm_mhz") or 1965.0
+    fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12  # nominal FMA rate at the sampled clock
     line = {
         "metric": METRIC, "value": world * n / (ms_mixed / 1e3) / 1e6, "unit": "Mpoints/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_mixed, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "n_points": n, "kernel": 111, "np": 6, "ptsmax": 64, "maxlevel": 10,
-                   "precision": "mixed (FP32 sums and spectra, FP64 pseudo-inverse products)", "rhs": 1,
+                   "precision": "mixed (FP32 point sums, spectra and Hadamard; surface contractions in split "
+                                "TF32 on tcgen05 with FP32 accumulation; FP64 operator SVDs)", "rhs": 1,
                    "l2": "flushed (256 MB write) before every timed step", "parallelism": f"replicas x{world}"},
         "relerr": relerr, "check_targets": NCHK,
         "fp64": fp64,
@@ -434,10 +441,13 @@ def engine_arm(args):
         "phases_ms": phases,
         "work": wc,
         "setup_s": setup_mixed,
-        "roofline": {"bound": "hbm", "kernel": "k_m2l_had (V-list Hadamard accumulate)", "achieved": achieved,
-                     "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind,
-                     "traffic": None, "kernel_ms": had_ms,
-                     "fp32_tflops": had_flops / (had_ms / 1e3) / 1e12},
+        "roofline": {"bound": "hbm", "kernel": "k_m2l_had_sweep (V-list Hadamard accumulate)",
+                     "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "peak_kind": peak_kind, "traffic": traffic, "traffic_unit": "bytes per launch",
+                     "kernel_ms": had_ms, "limiter": "FP32 FMA issue (fields below); DRAM traffic is 1.02x the "
+                                                     "algorithmic bytes",
+                     "fp32_tflops": had_flops / (had_ms / 1e3) / 1e12, "fp32_peak_tflops_nominal": fp32_peak,
+                     "fp32_frac": had_flops / (had_ms / 1e3) / 1e12 / fp32_peak},
         "clocks": clk,
         "cpu_baseline": cpu,
     }
