@@ -686,45 +686,28 @@ __device__ __forceinline__ void sweep_tile(const Cpx<T>* __restrict__ Ks, const 
     const int* cq[QPT];
 #pragma unroll
     for (int q = 0; q < QPT; q++) cq[q] = coll + (size_t)min(q0 + q, qend - 1) * 26;
-    int nb[QPT];
-    T nxr[QPT][8], nxi[QPT][8];
-#pragma unroll
-    for (int q = 0; q < QPT; q++) {
-      nb[q] = (q0 + q < qend) ? cq[q][0] : zero_node;
-      const Cpx<T>* X = spectra + ((size_t)nb[q] * SD + sc) * NF + fl;
-#pragma unroll
-      for (int j = 0; j < 8; j++) {
-        Cpx<T> x = X[j * XS];
-        nxr[q][j] = x.re;
-        nxi[q][j] = x.im;
-      }
-    }
-    for (int dir = 0; dir < 26; dir++) {
-      T xr[QPT][8], xi[QPT][8];
-      bool any = false;
+    // two register sets of colleague child spectra, alternating over the 26
+    // directions: set B is loaded while set A is multiplied and vice versa
+    int nbA[QPT], nbB[QPT];
+    T axr[QPT][8], axi[QPT][8], bxr[QPT][8], bxi[QPT][8];
+    auto load = [&](int dir, int* nb, T (*xr)[8], T (*xi)[8]) {
 #pragma unroll
       for (int q = 0; q < QPT; q++) {
-        any |= nb[q] != zero_node;
+        nb[q] = (q0 + q < qend) ? cq[q][dir] : zero_node;
+        const Cpx<T>* X = spectra + ((size_t)nb[q] * SD + sc) * NF + fl;
 #pragma unroll
         for (int j = 0; j < 8; j++) {
-          xr[q][j] = nxr[q][j];
-          xi[q][j] = nxi[q][j];
+          const Cpx<T> x = X[j * XS];
+          xr[q][j] = x.re;
+          xi[q][j] = x.im;
         }
       }
-      if (dir + 1 < 26) {
+    };
+    auto mult = [&](int dir, const int* nb, T (*xr)[8], T (*xi)[8]) {
+      bool any = false;
 #pragma unroll
-        for (int q = 0; q < QPT; q++) {
-          nb[q] = (q0 + q < qend) ? cq[q][dir + 1] : zero_node;
-          const Cpx<T>* X = spectra + ((size_t)nb[q] * SD + sc) * NF + fl;
-#pragma unroll
-          for (int j = 0; j < 8; j++) {
-            Cpx<T> x = X[j * XS];
-            nxr[q][j] = x.re;
-            nxi[q][j] = x.im;
-          }
-        }
-      }
-      if (!any) continue;
+      for (int q = 0; q < QPT; q++) any |= nb[q] != zero_node;
+      if (!any) return;
       // offset of child j of P from child i of Q: 2*dir + oct(j) - oct(i); the
       // adjacent pairs (|offset| <= 1) read the zero rows of the tile
       const Cpx<T>* Kd = Ks + c_dir_base[dir] * 32 + lane;
@@ -742,6 +725,13 @@ __device__ __forceinline__ void sweep_tile(const Cpx<T>* __restrict__ Ks, const 
           }
         }
       }
+    };
+    load(0, nbA, axr, axi);
+    for (int dir = 0; dir < 26; dir += 2) {
+      load(dir + 1, nbB, bxr, bxi);
+      mult(dir, nbA, axr, axi);
+      if (dir + 2 < 26) load(dir + 2, nbA, axr, axi);
+      mult(dir + 1, nbB, bxr, bxi);
     }
     if (f < NF) {
 #pragma unroll
