@@ -103,7 +103,8 @@ struct Impl : ImplBase {
   int ru = 0, rd = 0;  // ranks rounded up to multiples of 8 (zero-padded rows / columns)
   bool use_tc = false;
   T* khat;
-  T* ktiles = nullptr;  // [ceil(nf/32)][343][32] operator spectra for the parent-pair sweep
+  T* ktiles = nullptr;  // [td][sd][ceil(nf/32)][343][32] operator spectra for the parent-pair sweep
+  T* ttiles = nullptr;  // [td][sd][ceil(nf/16)][26][27][16] Toeplitz-factored operator
   int* h_status = nullptr;  // mapped host word: device-side wait time-outs (bit 0 sweep, bit 1 GEMM)
   int* d_status = nullptr;
   List s2m, s2l, leaf, m2l, fwd;
@@ -206,7 +207,11 @@ struct Impl : ImplBase {
                 kt[dst] = kh[src];
                 kt[dst + 1] = kh[src + 1];
               }
-        ktiles = upload(kt);
+        if (E.m2l_toeplitz) {
+          ttiles = upload(toeplitz_tables());
+        } else {
+          ktiles = upload(kt);
+        }
       }
     }
     KCHECK(cudaHostAlloc((void**)&h_status, sizeof(int), cudaHostAllocMapped));
@@ -312,7 +317,7 @@ struct Impl : ImplBase {
       spectra = dalloc<T>((size_t)(nn + 8) * sd_m * op.nfc * 2);
       KCHECK(cudaMemset(spectra, 0, sizeof(T) * (size_t)(nn + 8) * sd_m * op.nfc * 2));
       counters_v = (double)idx.size();
-      if (ktiles) build_pairs(work);
+      if (ktiles || ttiles) build_pairs(work);
       counters_fwd = (double)fwdn.size();
       counters_inv = (double)work.size();
     }
@@ -397,12 +402,9 @@ struct Impl : ImplBase {
     o.a = upload_as_T(A);
     if constexpr (sizeof(T) == 4) {
       if (use_tc && M % 4 == 0 && K % 4 == 0) {
-        std::vector<float> hi, lo;
-        split_tf32(M, K, A.data(), &hi, &lo, &o.tc.Np, &o.tc.Kp);
-        o.tc.hi = upload(hi);
-        o.tc.lo = upload(lo);
-        o.tc.M = M;
-        o.tc.K = K;
+        std::vector<float> img;
+        tc_operator_images(M, K, A.data(), &img, &o.tc);
+        o.tc.img = upload(img);
       }
     }
     return o;
@@ -441,6 +443,45 @@ struct Impl : ImplBase {
     op_dnW = make_op(dnW, rd, Kdc);
     op_dnV = make_op(dnV, K1, rd);
     op_l2lz = make_op(l2lz, 8 * rd, rd);
+  }
+
+  // Transformed operator of the Toeplitz-factored Hadamard: for direction d
+  // (components d = (dd/9-1, dd/3%3-1, dd%3-1), dd skipping the centre) and
+  // k = (kx, ky, kz) in {A, B, C}^3, T_k = sum over delta in {-1,0,1}^3 of
+  // c_kx(dx) c_ky(dy) c_kz(dz) K(2d + delta), with c_A = [delta = 0],
+  // c_B = [delta = 1] - [delta = 0], c_C = [delta = -1] - [delta = 0];
+  // in FP64 from the operator spectra, rounded once.
+  std::vector<T> toeplitz_tables() const {
+    const int nf = op.nfc, ft16 = (nf + 15) / 16, tsd = td_m * sd_m;
+    std::vector<T> out((size_t)tsd * ft16 * 26 * 28 * 16 * 2, T(0));  // [ts][tile][dir][k/2][16][k%2]
+    auto coef = [](int k, int d) -> double {
+      if (k == 0) return d == 0 ? 1.0 : 0.0;
+      if (k == 1) return (d == 1 ? 1.0 : 0.0) - (d == 0 ? 1.0 : 0.0);
+      return (d == -1 ? 1.0 : 0.0) - (d == 0 ? 1.0 : 0.0);
+    };
+    for (int dir = 0; dir < 26; dir++) {
+      const int dd = dir < 13 ? dir : dir + 1;
+      const int dv[3] = {dd / 9 - 1, (dd / 3) % 3 - 1, dd % 3 - 1};
+      for (int k = 0; k < 27; k++) {
+        const int kx = k / 9, ky = (k / 3) % 3, kz = k % 3;
+        for (int ts = 0; ts < tsd; ts++)
+          for (int f = 0; f < nf; f++) {
+            std::complex<double> acc(0.0, 0.0);
+            for (int ex = -1; ex <= 1; ex++)
+              for (int ey = -1; ey <= 1; ey++)
+                for (int ez = -1; ez <= 1; ez++) {
+                  const double c = coef(kx, ex) * coef(ky, ey) * coef(kz, ez);
+                  if (c == 0.0) continue;
+                  const int o = offset_index(2 * dv[0] + ex, 2 * dv[1] + ey, 2 * dv[2] + ez);
+                  acc += c * op.m2l[((size_t)o * tsd + ts) * nf + f];
+                }
+            const size_t dst = ((((((size_t)ts * ft16 + f / 16) * 26 + dir) * 14 + k / 2) * 16 + f % 16) * 2 + k % 2) * 2;
+            out[dst] = (T)acc.real();
+            out[dst + 1] = (T)acc.imag();
+          }
+      }
+    }
+    return out;
   }
 
   // Parent-pair form of the V list (single-dof equivalent kernels): one work
@@ -526,7 +567,7 @@ struct Impl : ImplBase {
     s.col_lvl = col_lvl;
     s.lvl_base = E.rootlvl;
     if constexpr (sizeof(T) == 4) {
-      if (A.tc.hi && ldb % 4 == 0 && ldc % 4 == 0) {
+      if (A.tc.img && ldb % 4 == 0 && ldc % 4 == 0) {
         nlaunch += launch_node_gemm_tc(A.tc, B, ldb, bidx, C, ldc, cidx, ncol, acc, s, gemm_ws, gemm_ws_len, num_sms,
                                        d_status, st);
         return;
@@ -576,8 +617,12 @@ struct Impl : ImplBase {
         launch_m2l_forward<T>(geom, supeden, fwd.work, fwd.n, d_depth, spectra, st);
         if (prof && r == 0) KCHECK(cudaEventRecord(ev[7], st));
         if (pairs_n > 0)
-          launch_m2l_hadamard_sweep<T>(op.nfc, sd_m, td_m, ktiles, spectra, pairs_n, pairs_chd, pairs_coll,
-                                       pairs_mask, effval, tr.nnodes, d_status, num_sms, st);
+          if (ttiles)
+            launch_m2l_hadamard_tz<T>(op.nfc, sd_m, td_m, ttiles, spectra, pairs_n, pairs_chd, pairs_coll, pairs_mask,
+                                      effval, tr.nnodes, d_status, num_sms, st);
+          else
+            launch_m2l_hadamard_sweep<T>(op.nfc, sd_m, td_m, ktiles, spectra, pairs_n, pairs_chd, pairs_coll,
+                                         pairs_mask, effval, tr.nnodes, d_status, num_sms, st);
         else
           launch_m2l_hadamard<T>(geom, khat, spectra, m2l.work, m2l.n, m2l.ptr, m2l.idx, d_path, effval, st);
         if (prof && r == 0) KCHECK(cudaEventRecord(ev[8], st));
@@ -723,6 +768,23 @@ int Engine::setup() {
       return KIFMM_ERR_OPTION;
     }
     tensor_cores = tc != 0;
+    auto fit = opts.find("-" + prefix + "m2l_form");
+    // default: the factored form in mixed precision (as fast as the direct form
+    // with ~40 % fewer multiply-adds), the direct form in FP64 (faster there)
+    m2l_toeplitz = mixed;
+    if (fit != opts.end()) {
+      std::string v = fit->second;
+      v.erase(0, v.find_first_not_of(" \t"));
+      v = v.substr(0, v.find_first_of(" \t%"));
+      if (v == "direct")
+        m2l_toeplitz = false;
+      else if (v == "toeplitz")
+        m2l_toeplitz = true;
+      else {
+        err = "m2l_form must be toeplitz or direct";
+        return KIFMM_ERR_OPTION;
+      }
+    }
   }
   if (!equivalent_kernel(user, &mm)) {
     err = "kernel not supported by FMM3d";

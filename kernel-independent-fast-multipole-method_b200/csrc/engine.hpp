@@ -40,6 +40,7 @@ struct Engine {
   int np = 6, ptsmax = 150, maxlevel = 10;
   bool mixed = false;
   bool tensor_cores = true;  // mixed mode: surface contractions on tcgen05 (split TF32)
+  bool m2l_toeplitz = false;  // V-list Hadamard in the 2x2x2 block-Toeplitz factored form
   bool profiling = false;
   // state
   bool ready = false;       // device state built, eval allowed

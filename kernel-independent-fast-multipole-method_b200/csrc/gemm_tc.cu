@@ -9,14 +9,16 @@
 // chunks of 32: the CTA's threads gather the 128 node columns (each a
 // contiguous K-vector) with 16-byte loads, split every value into a TF32 head
 // and a TF32 tail and store both into shared memory in the no-swizzle K-major
-// core-matrix layout; the operator chunk (split once on the host) arrives by
-// cp.async.  One thread then issues, per K-step of 8,
+// core-matrix layout; the operator chunk (split and laid out once on the
+// host) arrives as one bulk asynchronous copy on an mbarrier.  One thread
+// then issues, per K-step of 8,
 //   D += A_hi B_hi,  D += A_hi B_lo,  D += A_lo B_hi
 // into a fresh TMEM accumulator per chunk and commits them to an mbarrier.
 // Two accumulators alternate: while the MMAs of chunk c run, the threads
 // drain chunk c-1's accumulator (tcgen05.ld) into FP32 register sums and
-// load chunk c+1's node columns.  The epilogue applies the homogeneous level
-// scaling of the node and stores (or adds) 16-byte vectors.
+// load chunk c+2's node columns.  The epilogue stages the 128 x N tile in
+// shared memory, then writes whole output rows with coalesced 16-byte
+// stores, applying the homogeneous level scaling of each node.
 //
 // Precision: each product carries head*head exactly and the two cross terms
 // to TF32 accuracy (tail*tail, 2^-22 relative, is dropped).  The tensor core
@@ -42,6 +44,8 @@ constexpr int TC_TMEM_COLS = 512;     // two accumulators of up to 160 columns
 constexpr unsigned A_BYTES = TC_M * TC_KC * 4;        // 16 KB per head / tail
 constexpr unsigned B_BYTES = TC_NMAX * TC_KC * 4;     // 20 KB per head / tail
 constexpr unsigned A_STAGE = 2 * A_BYTES, B_STAGE = 2 * B_BYTES;
+constexpr int IMG_FLOATS = 2 * TC_NMAX * TC_KC;  // one operator chunk image: head + tail
+constexpr int OUT_LD = TC_NMAX + 4;               // staged output row stride (floats)
 // node tiles double-buffered, operator chunks triple-buffered: 184 KB, so one
 // CTA per SM, which owns all 512 TMEM columns
 constexpr unsigned TC_SMEM = 2 * A_STAGE + 3 * B_STAGE;
@@ -94,10 +98,6 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned parity)
   return false;
 }
 
-__device__ __forceinline__ void cp_async16(unsigned dst, const void* src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
-}
-
 __device__ __forceinline__ void mma_tf32(unsigned d, uint64_t a, uint64_t b, unsigned idesc, int acc) {
   asm volatile(
       "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(d),
@@ -123,23 +123,34 @@ __device__ __forceinline__ float pow2f(int e) {
   return (e >= -126 && e <= 127) ? __int_as_float((e + 127) << 23) : ldexpf(1.0f, e);
 }
 
+__device__ __forceinline__ void bulk_load(unsigned dst, const void* src, unsigned bytes, unsigned bar) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+
 __global__ void __launch_bounds__(TC_THREADS, 1) k_node_gemm_tc(TcOperator A, const float* __restrict__ B,
                                                                int64_t ldb, const int* __restrict__ bidx,
                                                                float* __restrict__ C, int64_t ldc,
                                                                const int* __restrict__ cidx, int ncol, int accumulate,
-                                                               GemmScale sc, int ntile, int kper,
-                                                               double* __restrict__ partial, int* __restrict__ status) {
+                                                               GemmScale sc, int kper, double* __restrict__ partial,
+                                                               int* __restrict__ status) {
   extern __shared__ __align__(1024) unsigned char smem[];
-  __shared__ __align__(8) unsigned long long bar[2];
+  __shared__ __align__(8) unsigned long long bar[2];  // MMA completion, per accumulator
+  __shared__ __align__(8) unsigned long long opb[3];  // operator chunk arrival, per B stage
   __shared__ unsigned tmem_base;
+  __shared__ int op_fail;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int n0 = blockIdx.y * ntile;
-  const int nn = min(ntile, A.Np - n0);  // rows of this tile (multiple of 16, <= 160)
-  const int half = nn / 2;               // columns per draining thread (multiple of 8)
+  const int n0 = blockIdx.y * A.ntile;
+  const int nn = min(A.ntile, A.Np - n0);  // rows of this tile (multiple of 16, <= 160)
+  const int half = nn / 2;                 // columns per draining thread (multiple of 8)
   const int col0 = blockIdx.x * TC_M;
+  const int nkt = A.Kp / TC_KC;
   // this CTA's K chunks (split K: blockIdx.z)
-  const int kb = blockIdx.z * kper, ke = min(A.Kp / TC_KC, kb + kper);
+  const int kb = blockIdx.z * kper, ke = min(nkt, kb + kper);
   const int nk = ke - kb;
+  const float* img = A.img + ((size_t)blockIdx.y * nkt + kb) * IMG_FLOATS;
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
@@ -148,8 +159,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_node_gemm_tc(TcOperator A, co
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   if (tid == 0) {
-    mbar_init(smem_u32(&bar[0]), 1);
-    mbar_init(smem_u32(&bar[1]), 1);
+    for (int b = 0; b < 2; b++) mbar_init(smem_u32(&bar[b]), 1);
+    for (int b = 0; b < 3; b++) mbar_init(smem_u32(&opb[b]), 1);
+    op_fail = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -159,18 +171,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_node_gemm_tc(TcOperator A, co
 
   auto a_stage = [&](int i) { return smem + (i & 1) * A_STAGE; };
   auto b_stage = [&](int i) { return smem + 2 * A_STAGE + (i % 3) * B_STAGE; };
-  // operator chunk i (local) -> its B stage, head and tail; one cp.async group
+  // operator chunk i (local): one bulk copy of its head + tail image
   auto issue_op = [&](int i) {
-    if (i < nk) {
-      unsigned char* bh = b_stage(i);
-      for (int e = tid; e < nn * 8; e += TC_THREADS) {
-        const int r = e >> 3, q = e & 7;
-        const size_t g = (size_t)(n0 + r) * A.Kp + (size_t)(kb + i) * TC_KC + 4 * q;
-        cp_async16(smem_u32(bh + core_off(r, q)), A.hi + g);
-        cp_async16(smem_u32(bh + B_BYTES + core_off(r, q)), A.lo + g);
-      }
-    }
-    asm volatile("cp.async.commit_group;" ::: "memory");
+    if (tid == 0 && i < nk)
+      bulk_load(smem_u32(b_stage(i)), img + (size_t)i * IMG_FLOATS, IMG_FLOATS * 4, smem_u32(&opb[i % 3]));
   };
   // node data: row (tid & 127) of the tile, column groups 4*(tid >> 7) .. +4
   const int lrow = tid & (TC_M - 1), lq0 = (tid >> 7) * 4;
@@ -231,22 +235,24 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_node_gemm_tc(TcOperator A, co
       *reinterpret_cast<float4*>(as + core_off(lrow, lq0 + q)) = h;
       *reinterpret_cast<float4*>(as + A_BYTES + core_off(lrow, lq0 + q)) = l;
     }
-    asm volatile("cp.async.wait_group 1;" ::: "memory");  // chunk i's operator (only i + 1 may be pending)
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
     if (tid == 0) {
+      if (!mbar_wait_bounded(smem_u32(&opb[i % 3]), (i / 3) & 1)) op_fail = 1;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const unsigned d = tmem + (unsigned)((i & 1) * TC_NMAX);
       const unsigned ah0 = smem_u32(as), al0 = ah0 + A_BYTES;
       const unsigned bh0 = smem_u32(b_stage(i)), bl0 = bh0 + B_BYTES;
+      if (!op_fail) {
 #pragma unroll
-      for (int s = 0; s < TC_KC / 8; s++) {
-        const unsigned off = s * 256;  // two core matrices along K per MMA
-        const uint64_t ah = smem_desc(ah0 + off), al = smem_desc(al0 + off);
-        const uint64_t bh = smem_desc(bh0 + off), bl = smem_desc(bl0 + off);
-        mma_tf32(d, ah, bh, idesc, s != 0);  // a fresh accumulator per chunk
-        mma_tf32(d, ah, bl, idesc, 1);
-        mma_tf32(d, al, bh, idesc, 1);
+        for (int s = 0; s < TC_KC / 8; s++) {
+          const unsigned off = s * 256;  // two core matrices along K per MMA
+          const uint64_t ah = smem_desc(ah0 + off), al = smem_desc(al0 + off);
+          const uint64_t bh = smem_desc(bh0 + off), bl = smem_desc(bl0 + off);
+          mma_tf32(d, ah, bh, idesc, s != 0);  // a fresh accumulator per chunk
+          mma_tf32(d, ah, bl, idesc, 1);
+          mma_tf32(d, al, bh, idesc, 1);
+        }
       }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                        smem_u32(&bar[i & 1]))
@@ -256,7 +262,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_node_gemm_tc(TcOperator A, co
     if (i > 0) {
       // chunk i-1's MMAs: their A / B stages and accumulator become free
       const bool done = mbar_wait_bounded(smem_u32(&bar[(i - 1) & 1]), ((i - 1) >> 1) & 1);
-      if (__syncthreads_or(!done)) return false;
+      if (__syncthreads_or(!done || op_fail)) return false;
       drain((i - 1) & 1);
     }
     issue_op(i + 2);  // into the stage chunk i-1 used
@@ -268,43 +274,47 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_node_gemm_tc(TcOperator A, co
   }
   if (ok && nk > 0) {
     const bool done = mbar_wait_bounded(smem_u32(&bar[(nk - 1) & 1]), ((nk - 1) >> 1) & 1);
-    ok = !__syncthreads_or(!done);
+    ok = !__syncthreads_or(!done || op_fail);
     if (ok) drain((nk - 1) & 1);
   }
-  asm volatile("cp.async.wait_group 0;" ::: "memory");
   if (ok) {
-    // lane of this thread = node row (warp & 3) * 32 + lane; columns of its half
-    const int j = col0 + (warp & 3) * 32 + lane;
-    const int nb = n0 + (warp >> 2) * half;
-    if (j < ncol && partial) {  // split K: raw sums, scaled and added by the reduce
-      double* pr = partial + ((size_t)blockIdx.z * ncol + j) * A.M;
+    // stage the tile: row (warp & 3) * 32 + lane, columns of this thread's half
+    __syncthreads();  // every MMA has completed: the operand stages are free
+    float* out = reinterpret_cast<float*>(smem);
+    {
+      float* orow = out + ((warp & 3) * 32 + lane) * OUT_LD + (warp >> 2) * half;
 #pragma unroll
-      for (int i = 0; i < TC_HALF; i++)
-        if (i < half && nb + i < A.M) pr[nb + i] = (double)sum[i];
-    } else if (j < ncol) {
-      float* crow = C + (int64_t)cidx[j] * ldc;
-      const int lvl = sc.col_lvl ? sc.col_lvl[j] + sc.lvl_base : 0;
-      float f4[4];  // scale of output n: f4[n % sd], sd <= 4
-#pragma unroll
-      for (int d = 0; d < 4; d++) f4[d] = sc.col_lvl ? pow2f(-lvl * sc.deg[d < sc.sd ? d : 0]) : 1.0f;
-#pragma unroll
-      for (int i = 0; i < TC_HALF; i += 4) {
-        const int n = nb + i;
-        if (i >= half || n >= A.M) break;
-        float4 o = make_float4(sum[i], sum[i + 1], sum[i + 2], sum[i + 3]);
+      for (int i = 0; i < TC_HALF; i += 4)
+        if (i < half) *reinterpret_cast<float4*>(orow + i) = make_float4(sum[i], sum[i + 1], sum[i + 2], sum[i + 3]);
+    }
+    __syncthreads();
+    const int nv = min(nn, A.M - n0);  // valid output rows of this N tile (multiple of 4)
+    const int nv4 = nv / 4;
+    const int rows = min(TC_M, ncol - col0);
+    if (partial) {  // split K: raw sums, scaled and added by the reduce
+      for (int e = tid; e < rows * nv; e += TC_THREADS) {
+        const int r = e / nv, c = e - r * nv;
+        partial[((size_t)blockIdx.z * ncol + col0 + r) * A.M + n0 + c] = (double)out[r * OUT_LD + c];
+      }
+    } else {
+      for (int e = tid; e < rows * nv4; e += TC_THREADS) {
+        const int r = e / nv4, c = e - r * nv4;
+        const int j = col0 + r, n = n0 + 4 * c;
+        float4 o = *reinterpret_cast<const float4*>(out + r * OUT_LD + 4 * c);
         if (sc.col_lvl) {
-          o.x *= f4[(n + 0) % sc.sd];
-          o.y *= f4[(n + 1) % sc.sd];
-          o.z *= f4[(n + 2) % sc.sd];
-          o.w *= f4[(n + 3) % sc.sd];
+          const int lvl = sc.col_lvl[j] + sc.lvl_base;
+          o.x *= pow2f(-lvl * sc.deg[(n + 0) % sc.sd]);
+          o.y *= pow2f(-lvl * sc.deg[(n + 1) % sc.sd]);
+          o.z *= pow2f(-lvl * sc.deg[(n + 2) % sc.sd]);
+          o.w *= pow2f(-lvl * sc.deg[(n + 3) % sc.sd]);
         }
-        float4* p = reinterpret_cast<float4*>(crow + n);
+        float4* p = reinterpret_cast<float4*>(C + (int64_t)cidx[j] * ldc + n);
         if (accumulate) {
-          const float4 c = *p;
-          o.x += c.x;
-          o.y += c.y;
-          o.z += c.z;
-          o.w += c.w;
+          const float4 c4 = *p;
+          o.x += c4.x;
+          o.y += c4.y;
+          o.z += c4.z;
+          o.w += c4.w;
         }
         *p = o;
       }
@@ -330,17 +340,34 @@ inline float tf32_round_host(float x) {
 
 }  // namespace
 
-void split_tf32(int M, int K, const double* A, std::vector<float>* hi, std::vector<float>* lo, int* Np, int* Kp) {
-  *Np = (M + 15) / 16 * 16;
-  *Kp = (K + TC_KC - 1) / TC_KC * TC_KC;
-  hi->assign((size_t)*Np * *Kp, 0.f);
-  lo->assign((size_t)*Np * *Kp, 0.f);
-  for (int r = 0; r < M; r++)
-    for (int k = 0; k < K; k++) {
-      const double a = A[(size_t)r * K + k];
-      const float h = tf32_round_host((float)a);
-      (*hi)[(size_t)r * *Kp + k] = h;
-      (*lo)[(size_t)r * *Kp + k] = tf32_round_host((float)(a - (double)h));
+void tc_operator_images(int M, int K, const double* A, std::vector<float>* img, TcOperator* d) {
+  d->M = M;
+  d->K = K;
+  d->Np = (M + 15) / 16 * 16;
+  d->Kp = (K + TC_KC - 1) / TC_KC * TC_KC;
+  // balanced N tiles of at most 160 rows, multiples of 16
+  const int nt_count = (d->Np + TC_NMAX - 1) / TC_NMAX;
+  d->ntile = ((d->Np + nt_count - 1) / nt_count + 15) / 16 * 16;
+  d->ntiles = (d->Np + d->ntile - 1) / d->ntile;
+  const int nkt = d->Kp / TC_KC;
+  img->assign((size_t)d->ntiles * nkt * IMG_FLOATS, 0.f);
+  for (int y = 0; y < d->ntiles; y++)
+    for (int c = 0; c < nkt; c++) {
+      float* base = img->data() + ((size_t)y * nkt + c) * IMG_FLOATS;
+      for (int r = 0; r < d->ntile; r++) {
+        const int n = y * d->ntile + r;
+        if (n >= M) break;
+        for (int k = 0; k < TC_KC; k++) {
+          const int kk = c * TC_KC + k;
+          if (kk >= K) break;
+          const double a = A[(size_t)n * K + kk];
+          const float h = tf32_round_host((float)a);
+          const float l = tf32_round_host((float)(a - (double)h));
+          const size_t off = (size_t)(((r >> 3) * 8 + (k >> 2)) * 32 + (r & 7) * 4 + (k & 3));
+          base[off] = h;
+          base[TC_NMAX * TC_KC + off] = l;
+        }
+      }
     }
 }
 
@@ -348,10 +375,7 @@ int launch_node_gemm_tc(const TcOperator& A, const float* B, int64_t ldb, const 
                         const int* cidx, int ncol, bool accumulate, const GemmScale& sc, double* ws, size_t ws_len,
                         int num_sms, int* status, cudaStream_t st) {
   if (ncol <= 0 || A.M <= 0 || A.K <= 0) return 0;
-  // balanced N tiles of at most 160 rows, multiples of 16
-  const int nt_count = (A.Np + TC_NMAX - 1) / TC_NMAX;
-  const int ntile = ((A.Np + nt_count - 1) / nt_count + 15) / 16 * 16;
-  const int gx = (ncol + TC_M - 1) / TC_M, gy = (A.Np + ntile - 1) / ntile;
+  const int gx = (ncol + TC_M - 1) / TC_M, gy = A.ntiles;
   const int nk = A.Kp / TC_KC;
   // few tiles (the shallow tree levels): split K so that every SM has work
   int splits = 1;
@@ -364,8 +388,8 @@ int launch_node_gemm_tc(const TcOperator& A, const float* B, int64_t ldb, const 
   splits = (nk + kper - 1) / kper;
   dim3 grid(gx, gy, splits);
   cudaFuncSetAttribute(k_node_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM);
-  k_node_gemm_tc<<<grid, TC_THREADS, TC_SMEM, st>>>(A, B, ldb, bidx, C, ldc, cidx, ncol, accumulate ? 1 : 0, sc, ntile,
-                                                     kper, splits > 1 ? ws : nullptr, status);
+  k_node_gemm_tc<<<grid, TC_THREADS, TC_SMEM, st>>>(A, B, ldb, bidx, C, ldc, cidx, ncol, accumulate ? 1 : 0, sc, kper,
+                                                     splits > 1 ? ws : nullptr, status);
   if (splits > 1) launch_node_gemm_reduce_f(A.M, ncol, splits, ws, C, ldc, cidx, accumulate, sc, num_sms, st);
   return splits > 1 ? 2 : 1;
 }

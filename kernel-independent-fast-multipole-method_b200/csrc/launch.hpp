@@ -75,22 +75,26 @@ int launch_node_gemm(int M, int K, const T* A, const T* B, int64_t ldb, const in
 
 // The same product on the tensor cores (tcgen05, kind::tf32) for FP32 data,
 // with both operands split into a TF32 head and a TF32 tail and three MMAs
-// (head*head + head*tail + tail*head) accumulating in FP32 in tensor memory:
-// about 2^-21 relative per product, the FP32 rounding class.  The operator is
-// pre-split on the host: hi/lo are Np x Kp row-major (Np = M rounded up to 16,
-// Kp = K rounded up to 32, zero padded).  Requires K, ldb, ldc multiples of 4
-// and 16-byte aligned B and C.  Launches with fewer tiles than SMs split K
-// over CTAs into ws (FP64, ws_len doubles) and reduce it deterministically.
-// A bounded wait that times out sets bit 1 of *status.  Returns the number
-// of launches.
+// (head*head + head*tail + tail*head) accumulating in FP32: about 2^-21
+// relative per product, the FP32 rounding class.  The operator is split on
+// the host into shared-memory images, one per (N tile, 32-wide K chunk):
+// head then tail, each 160 rows x 32 columns in the no-swizzle K-major
+// core-matrix layout (zero padded), so that one bulk copy moves a chunk.
+// Requires K, ldb, ldc multiples of 4 and 16-byte aligned B and C.  Launches
+// with fewer tiles than SMs split K over CTAs into ws (FP64, ws_len doubles)
+// and reduce it deterministically.  A bounded wait that times out sets bit 1
+// of *status.  Returns the number of launches.
 struct TcOperator {
-  const float* hi = nullptr;
-  const float* lo = nullptr;
+  const float* img = nullptr;  // [ntiles][Kp/32][2][160 x 32]
   int M = 0, K = 0, Np = 0, Kp = 0;
+  int ntile = 0, ntiles = 0;  // rows per N tile (multiple of 16, <= 160), number of N tiles
 };
 int launch_node_gemm_tc(const TcOperator& A, const float* B, int64_t ldb, const int* bidx, float* C, int64_t ldc,
                         const int* cidx, int ncol, bool accumulate, const GemmScale& sc, double* ws, size_t ws_len,
                         int num_sms, int* status, cudaStream_t st);
+// host side: the images of a row-major M x K operator (fills A's sizes; img
+// is left to the caller to upload)
+void tc_operator_images(int M, int K, const double* A, std::vector<float>* img, TcOperator* desc);
 // C[cidx[j]] (=|+=) scaled sum over nslice of partial[z][j][0..M) (gemm.cu)
 void launch_node_gemm_reduce_f(int M, int ncol, int nslice, const double* partial, float* C, int64_t ldc,
                                const int* cidx, bool accumulate, const GemmScale& sc, int num_sms, cudaStream_t st);
@@ -130,6 +134,15 @@ template <typename T>
 void launch_m2l_hadamard_sweep(int nf, int sd, int td, const T* ktiles, const T* spectra, int nq, const int* qchd,
                                const int* coll, const unsigned char* mask, T* effval, int zero_node, int* status,
                                int num_sms, cudaStream_t st);
+// The same product with the 2 x 2 x 2 block-Toeplitz factorisation of each
+// colleague block (27 instead of 64 complex products per direction).  ttiles:
+// [td][sd][ceil(nf/16)][26 directions][14][16][2] complex: for direction d
+// and frequency lane l, the 27 transformed values k (padded to 28) stored as
+// pairs (k, k+1) at [d][k/2][l][k%2].
+template <typename T>
+void launch_m2l_hadamard_tz(int nf, int sd, int td, const T* ttiles, const T* spectra, int nq, const int* qchd,
+                            const int* coll, const unsigned char* mask, T* effval, int zero_node, int* status,
+                            int num_sms, cudaStream_t st);
 // tdncval[node] += extract(inverse(effval[node]))
 template <typename T>
 void launch_m2l_inverse(const M2LGeom& g, const T* effval, const int* work, int nwork, T* tdncval,

@@ -837,6 +837,248 @@ __global__ void __launch_bounds__(NTHR) k_m2l_had_sweep(const Cpx<T>* __restrict
   }
 }
 
+// ---------------------------------------------------------------------------
+// Toeplitz-factored parent-pair Hadamard.  For one colleague direction d the
+// child-to-child block is M[i][j] = K(2d + oct(j) - oct(i)): along each axis a
+// 2 x 2 Toeplitz matrix [[t0, t1], [t-1, t0]], whose product needs three
+// multiplications instead of four:
+//   y0 = A + B, y1 = A + C,  A = t0 (x0 + x1), B = (t1 - t0) x1, C = (t-1 - t0) x0.
+// Over the three axes that is 27 products U_k T_k instead of 64.  The input
+// combinations U_k (x0 + x1, x1, x0 per axis) do not depend on d and the output
+// combination is linear, so each lane accumulates sum_d T_k(d) U_k(d) for all
+// 27 k and applies the output combination once per target parent.  Per
+// frequency and direction: 27 complex multiply-adds and 19 complex adds in
+// place of 64 complex multiply-adds.  The transformed operator T[d][k] (26 x 27
+// values per frequency, products of the differences above, formed in FP64 on
+// the host) is staged per tile of 16 frequencies; a warp carries two target
+// parents, one per half-warp, on the same 16 frequencies.
+constexpr int TZ_F = 16;          // frequencies per tile
+constexpr int TZ_ROWS = 26 * 28;  // transformed operator values per frequency (27 per direction, padded to 28)
+
+// two consecutive transformed operator values of one frequency: layout
+// [dir][k/2][16][2] lets one 16-byte shared load (FP32) fetch both
+template <typename T>
+struct __align__(4 * sizeof(T)) Cpx2 {
+  Cpx<T> a, b;
+};
+
+template <typename T>
+__device__ __forceinline__ void cadd(Cpx<T>& r, const Cpx<T>& a, const Cpx<T>& b) {
+  r.re = a.re + b.re;
+  r.im = a.im + b.im;
+}
+
+template <typename T, int NF, int SD, int TD>
+__device__ __forceinline__ void tz_tile(const Cpx<T>* __restrict__ Ts, const Cpx<T>* __restrict__ spectra,
+                                        int* claim, int qend, int f, const int* __restrict__ qchd,
+                                        const int* __restrict__ coll, const unsigned char* __restrict__ mask,
+                                        Cpx<T>* __restrict__ effval, int zero_node, int sc, int tc, bool acc_out) {
+  constexpr int XS = SD * NF;  // source child stride
+  const int lane = threadIdx.x & 31, hl = lane & 15, hw = lane >> 4;
+  const int fl = min(f, NF - 1);  // lanes past NF load a valid spectrum and store nothing
+  while (true) {
+    int q0 = 0;
+    if (lane == 0) q0 = atomicAdd(claim, 2);
+    q0 = __shfl_sync(0xffffffffu, q0, 0);
+    if (q0 >= qend) break;
+    const int q = q0 + hw;  // this half-warp's target parent
+    const bool qv = q < qend;
+    const int* cq = coll + (size_t)min(q, qend - 1) * 26;
+    Cpx<T> acc[27];
+#pragma unroll
+    for (int k = 0; k < 27; k++) acc[k].re = acc[k].im = T(0);
+    Cpx<T> xa[8], xb[8];
+    int nba, nbb;
+    auto load = [&](int dir, Cpx<T>* x, int& nb) {
+      nb = qv ? cq[dir] : zero_node;
+      const Cpx<T>* X = spectra + ((size_t)nb * SD + sc) * NF + fl;
+#pragma unroll
+      for (int j = 0; j < 8; j++) x[j] = X[j * XS];
+    };
+    auto mult = [&](int dir, const Cpx<T>* x, int nb) {
+      if (!__any_sync(0xffffffffu, nb != zero_node)) return;
+      const Cpx2<T>* Td = reinterpret_cast<const Cpx2<T>*>(Ts) + (size_t)dir * 14 * TZ_F + hl;
+      Cpx2<T> tp;
+      // child j = (jx, jy, jz) bits (2, 1, 0); per axis the combinations
+      // A = x(0) + x(1), B = x(1), C = x(0)
+#pragma unroll
+      for (int kx = 0; kx < 3; kx++) {
+        Cpx<T> v[4];  // [jy][jz]
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+          if (kx == 0) cadd(v[e], x[e], x[4 + e]);
+          else v[e] = kx == 1 ? x[4 + e] : x[e];
+        }
+#pragma unroll
+        for (int ky = 0; ky < 3; ky++) {
+          Cpx<T> w[2];  // [jz]
+#pragma unroll
+          for (int e = 0; e < 2; e++) {
+            if (ky == 0) cadd(w[e], v[e], v[2 + e]);
+            else w[e] = ky == 1 ? v[2 + e] : v[e];
+          }
+#pragma unroll
+          for (int kz = 0; kz < 3; kz++) {
+            Cpx<T> u;
+            if (kz == 0) cadd(u, w[0], w[1]);
+            else u = kz == 1 ? w[1] : w[0];
+            const int k = (kx * 3 + ky) * 3 + kz;
+            if ((k & 1) == 0) tp = Td[(k >> 1) * TZ_F];
+            const Cpx<T> t = (k & 1) ? tp.b : tp.a;
+            acc[k].re = fmt(-t.im, u.im, fmt(t.re, u.re, acc[k].re));
+            acc[k].im = fmt(t.im, u.re, fmt(t.re, u.im, acc[k].im));
+          }
+        }
+      }
+    };
+    load(0, xa, nba);
+    for (int dir = 0; dir < 26; dir += 2) {
+      load(dir + 1, xb, nbb);
+      mult(dir, xa, nba);
+      if (dir + 2 < 26) load(dir + 2, xa, nba);
+      mult(dir + 1, xb, nbb);
+    }
+    if (!qv || f >= NF) continue;
+    // output combination per axis: y(0) = A + B, y(1) = A + C
+    Cpx<T> r[18];  // [kx][ky][iz]
+#pragma unroll
+    for (int g = 0; g < 9; g++) {
+      cadd(r[2 * g], acc[3 * g], acc[3 * g + 1]);
+      cadd(r[2 * g + 1], acc[3 * g], acc[3 * g + 2]);
+    }
+    Cpx<T> s4[12];  // [kx][iy][iz]
+#pragma unroll
+    for (int kx = 0; kx < 3; kx++)
+#pragma unroll
+      for (int iz = 0; iz < 2; iz++) {
+        const Cpx<T> a0 = r[(kx * 3 + 0) * 2 + iz], b0 = r[(kx * 3 + 1) * 2 + iz], c0 = r[(kx * 3 + 2) * 2 + iz];
+        cadd(s4[(kx * 2 + 0) * 2 + iz], a0, b0);
+        cadd(s4[(kx * 2 + 1) * 2 + iz], a0, c0);
+      }
+    const int c0 = qchd[q];
+    const unsigned m = mask[q];
+#pragma unroll
+    for (int e = 0; e < 4; e++) {  // (iy, iz)
+      Cpx<T> y[2];
+      cadd(y[0], s4[0 * 4 + e], s4[1 * 4 + e]);
+      cadd(y[1], s4[0 * 4 + e], s4[2 * 4 + e]);
+#pragma unroll
+      for (int ix = 0; ix < 2; ix++) {
+        const int i = ix * 4 + e;
+        if (!((m >> i) & 1)) continue;
+        Cpx<T>* py = effval + ((size_t)(c0 + i) * TD + tc) * NF + f;
+        Cpx<T> v = y[ix];
+        if (acc_out) {
+          const Cpx<T> o = *py;
+          v.re += o.re;
+          v.im += o.im;
+        }
+        *py = v;
+      }
+    }
+  }
+}
+
+template <typename T, int NF, int NTHR, int NBUF, int SD, int TD>
+__global__ void __launch_bounds__(NTHR) k_m2l_had_tz(const Cpx<T>* __restrict__ ttiles,
+                                                    const Cpx<T>* __restrict__ spectra, int nq,
+                                                    const int* __restrict__ qchd, const int* __restrict__ coll,
+                                                    const unsigned char* __restrict__ mask,
+                                                    Cpx<T>* __restrict__ effval, int zero_node, int sc, int tc, int acc,
+                                                    int* __restrict__ status) {
+  constexpr int TILE = TZ_ROWS * TZ_F;
+  constexpr unsigned TILE_BYTES = TILE * sizeof(Cpx<T>);
+  constexpr int FTILES = (NF + TZ_F - 1) / TZ_F;
+  constexpr int NW = NTHR / 32;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Cpx<T>* Tbuf = reinterpret_cast<Cpx<T>*>(smem_raw);  // NBUF x [26][27][16]
+  __shared__ __align__(8) unsigned long long bars[NBUF];
+  __shared__ int claim[NBUF], done_cnt[NBUF];
+  const int lane = threadIdx.x & 31;
+  const int per_cta = (nq + gridDim.x - 1) / gridDim.x;
+  const int qbeg = blockIdx.x * per_cta;
+  const int qend = min(nq, qbeg + per_cta);
+  if (threadIdx.x == 0) {
+    for (int b = 0; b < NBUF; b++) {
+      mbar_init(smem_addr(&bars[b]), 1);
+      claim[b] = qbeg;
+      done_cnt[b] = 0;
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    if (NBUF == 2) {
+      bulk_load(smem_addr(Tbuf), ttiles, TILE_BYTES, smem_addr(&bars[0]));
+      if (FTILES > 1) bulk_load(smem_addr(Tbuf + TILE), ttiles + TILE, TILE_BYTES, smem_addr(&bars[1]));
+    }
+  }
+  __syncthreads();
+  if constexpr (NBUF == 2) {
+    for (int ft = 0; ft < FTILES; ft++) {
+      const int b = ft & 1;
+      const bool ok = mbar_wait_bounded(smem_addr(&bars[b]), (ft >> 1) & 1);
+      if (!ok) {
+        if (lane == 0) atomicOr(status, 1);
+        return;
+      }
+      tz_tile<T, NF, SD, TD>(Tbuf + (size_t)b * TILE, spectra, &claim[b], qend, ft * TZ_F + (lane & 15), qchd, coll,
+                             mask, effval, zero_node, sc, tc, acc != 0);
+      if (lane == 0) {
+        if (atomicAdd(&done_cnt[b], 1) == NW - 1) {  // the last warp out of tile ft
+          done_cnt[b] = 0;
+          claim[b] = qbeg;
+          if (ft + 2 < FTILES)
+            bulk_load(smem_addr(Tbuf + (size_t)b * TILE), ttiles + (size_t)(ft + 2) * TILE, TILE_BYTES,
+                      smem_addr(&bars[b]));
+        }
+      }
+      __syncwarp();
+    }
+  } else {
+    for (int ft = 0; ft < FTILES; ft++) {
+      if (threadIdx.x == 0) {
+        claim[0] = qbeg;
+        bulk_load(smem_addr(Tbuf), ttiles + (size_t)ft * TILE, TILE_BYTES, smem_addr(&bars[0]));
+      }
+      __syncthreads();
+      const bool ok = mbar_wait_bounded(smem_addr(&bars[0]), ft & 1);
+      if (__syncthreads_or(!ok)) {
+        if (threadIdx.x == 0) atomicOr(status, 1);
+        return;
+      }
+      tz_tile<T, NF, SD, TD>(Tbuf, spectra, &claim[0], qend, ft * TZ_F + (lane & 15), qchd, coll, mask, effval,
+                             zero_node, sc, tc, acc != 0);
+      __syncthreads();
+    }
+  }
+}
+
+template <typename T, int NF, int SD, int TD>
+void tz_launch(const T* ttiles, const T* spectra, int nq, const int* qchd, const int* coll, const unsigned char* mask,
+               T* effval, int zero_node, int* status, int num_sms, cudaStream_t st) {
+  constexpr int NTHR = sizeof(T) == 4 ? 512 : 256;
+  constexpr int NBUF = sizeof(T) == 4 ? 2 : 1;
+  const size_t smem = (size_t)NBUF * TZ_ROWS * TZ_F * sizeof(Cpx<T>);
+  auto kern = k_m2l_had_tz<T, NF, NTHR, NBUF, SD, TD>;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const int grid = std::max(1, std::min(num_sms, nq / 32));
+  const size_t tiles = (size_t)((NF + TZ_F - 1) / TZ_F) * TZ_ROWS * TZ_F;  // Cpx per (t, s) table
+  for (int t = 0; t < TD; t++)
+    for (int s = 0; s < SD; s++)
+      kern<<<grid, NTHR, smem, st>>>(reinterpret_cast<const Cpx<T>*>(ttiles) + (size_t)(t * SD + s) * tiles,
+                                     reinterpret_cast<const Cpx<T>*>(spectra), nq, qchd, coll, mask,
+                                     reinterpret_cast<Cpx<T>*>(effval), zero_node, s, t, s > 0 ? 1 : 0, status);
+}
+
+template <typename T, int NF>
+void tz_dofs(int sd, int td, const T* ttiles, const T* spectra, int nq, const int* qchd, const int* coll,
+             const unsigned char* mask, T* effval, int zero_node, int* status, int num_sms, cudaStream_t st) {
+  if (sd == 1 && td == 1)
+    tz_launch<T, NF, 1, 1>(ttiles, spectra, nq, qchd, coll, mask, effval, zero_node, status, num_sms, st);
+  else if (sd == 4 && td == 3)
+    tz_launch<T, NF, 4, 3>(ttiles, spectra, nq, qchd, coll, mask, effval, zero_node, status, num_sms, st);
+  else if (sd == 3 && td == 3)
+    tz_launch<T, NF, 3, 3>(ttiles, spectra, nq, qchd, coll, mask, effval, zero_node, status, num_sms, st);
+}
+
 template <typename T, int NF, int SD, int TD>
 void sweep_launch(const T* ktiles, const T* spectra, int nq, const int* qchd, const int* coll,
                   const unsigned char* mask, T* effval, int zero_node, int* status, int num_sms, cudaStream_t st) {
@@ -891,9 +1133,24 @@ void launch_m2l_hadamard_sweep(int nf, int sd, int td, const T* ktiles, const T*
     sweep_dofs<T, 2052>(sd, td, ktiles, spectra, nq, qchd, coll, mask, effval, zero_node, status, num_sms, st);
 }
 
+template <typename T>
+void launch_m2l_hadamard_tz(int nf, int sd, int td, const T* ttiles, const T* spectra, int nq, const int* qchd,
+                            const int* coll, const unsigned char* mask, T* effval, int zero_node, int* status,
+                            int num_sms, cudaStream_t st) {
+  if (nq <= 0) return;
+  if (nf == 868)
+    tz_dofs<T, 868>(sd, td, ttiles, spectra, nq, qchd, coll, mask, effval, zero_node, status, num_sms, st);
+  else if (nf == 260)
+    tz_dofs<T, 260>(sd, td, ttiles, spectra, nq, qchd, coll, mask, effval, zero_node, status, num_sms, st);
+  else if (nf == 2052)
+    tz_dofs<T, 2052>(sd, td, ttiles, spectra, nq, qchd, coll, mask, effval, zero_node, status, num_sms, st);
+}
+
 #define KIFMM_INST(T)                                                                                             \
   template void launch_m2l_hadamard_sweep<T>(int, int, int, const T*, const T*, int, const int*, const int*,     \
                                              const unsigned char*, T*, int, int*, int, cudaStream_t);              \
+  template void launch_m2l_hadamard_tz<T>(int, int, int, const T*, const T*, int, const int*, const int*,        \
+                                          const unsigned char*, T*, int, int*, int, cudaStream_t);                 \
   template void launch_m2l_forward<T>(const M2LGeom&, const T*, const int*, int, const int*, T*, cudaStream_t);  \
   template void launch_m2l_hadamard<T>(const M2LGeom&, const T*, const T*, const int*, int, const int64_t*,     \
                                        const int*, const int*, T*, cudaStream_t);                                \

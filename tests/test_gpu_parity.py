@@ -215,3 +215,28 @@ def test_mixed_tensor_core_contractions_match_simt(gpu, name):
         assert err <= max(10 * d["ref_relerr"], MIXED_FLOOR), (tc, err, d["ref_relerr"])
     diff = np.linalg.norm(outs[0] - outs[1]) / np.linalg.norm(outs[1])
     assert diff <= 1e-5, diff
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("mixed", 5e-6)])
+@pytest.mark.parametrize("name", ["lap_s_np6_tt_style", "stk_s_np6_cube", "lap_s_np4_sphere", "lap_s_np8_plummer"])
+def test_toeplitz_hadamard_matches_direct_form(gpu, name, precision, tol):
+    """The 2x2x2 block-Toeplitz factored V-list product (27 instead of 64
+    complex products per colleague direction) against the direct
+    parent-pair product: the same sums in another order, so they agree to
+    rounding (1e-12 relative in FP64, 5e-6 in mixed)."""
+    d = G.load(name)
+    td = W.KERNEL_DOFS[d["kt"]][1]
+    outs = []
+    for form in ("toeplitz", "direct"):
+        f = kifmm.FMM3d("fmm3d_")
+        f.srcpos, f.srcnor, f.trgpos = d["src"], d["nor"], d["trg"]
+        f.ctr, f.rootlvl = tuple(d["ctr"]), d["rootlvl"]
+        f.knl = kifmm.Kernel3d(d["kt"], d["coefs"])
+        o = G.options(d, precision)
+        o["-fmm3d_m2l_form"] = form
+        f.setup(o)
+        out = np.zeros(td * len(d["trg"]))
+        f.eval(d["den"], out)
+        outs.append(out)
+    diff = np.linalg.norm(outs[0] - outs[1]) / np.linalg.norm(outs[1])
+    assert diff <= tol, diff
