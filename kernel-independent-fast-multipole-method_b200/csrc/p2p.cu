@@ -1,19 +1,18 @@
 // Point <-> point and point <-> surface evaluation passes.
 //
-//   k_s2m   S2M  : leaf sources -> its upward check surface      (SE2UC_dgemv, fmm3d/fmm3d.cpp:62-71)
-//   k_s2l   S2L  : X-list leaf sources -> downward check surface  (SE2DC_dgemv, fmm3d/fmm3d.cpp:73-82)
-//   k_leaf  near : U list + direct W/X (SE2TC_dgemv, fmm3d/fmm3d.cpp:35-60), M2T from W-list
-//                  upward equivalent surfaces (UE2TC_dgemv, :114-141) and L2T from the leaf's own
-//                  downward equivalent surface (DE2TC_dgemv, :84-112), fused into one pass that
-//                  writes each target once.
-//   k_direct     : FP64 direct sum (Dense3d::eval, fmm3d/dense3d.cpp:38-57).
+//   k_s2m_warp   S2M  : leaf sources -> its upward check surface      (SE2UC_dgemv, fmm3d/fmm3d.cpp:62-71)
+//   k_s2l        S2L  : X-list leaf sources -> downward check surface  (SE2DC_dgemv, fmm3d/fmm3d.cpp:73-82)
+//   k_leaf_warp  near : U list + direct W/X (SE2TC_dgemv, fmm3d/fmm3d.cpp:35-60), M2T from W-list
+//                       upward equivalent surfaces (UE2TC_dgemv, :114-141) and L2T from the leaf's own
+//                       downward equivalent surface (DE2TC_dgemv, :84-112), fused into one pass that
+//                       writes each target once.
+//   k_direct          : FP64 direct sum (Dense3d::eval, fmm3d/dense3d.cpp:38-57).
 //
-// One CTA per work node.  Sources are staged through shared memory in tiles
-// and every target accumulates in registers; when a node has few targets the
-// CTA's threads split the source tile among several groups per target and
-// reduce through shared memory at the end.  Positions are stored relative to
-// the centre of their leaf and re-centred on the target node's centre while
-// staging, so FP32 differences lose no more than the node size's precision.
+// S2M and the leaf pass run one warp per leaf (see below); S2L, rare, one CTA
+// per node with shared-memory tiles.  Every target accumulates in registers.
+// Positions are stored relative to the centre of their leaf and re-centred on
+// the target node's centre while staging, so FP32 differences lose no more
+// than the node size's precision.
 #include "kernels_common.cuh"
 #include "launch.hpp"
 
@@ -36,70 +35,12 @@ struct Red {
   T v[P2P_THREADS * TDMAX];
 };
 
-// Packed source tile: p[j] = (x, y, z, first density component); further
-// density components in f (SD-1 per point) and normals in n (double layer).
-// A single-dof single-layer interaction then reads one 16-byte (FP32) word.
+// Packed staged source: (x, y, z, first density component); a single-dof
+// single-layer interaction then reads one 16-byte (FP32) word.
 template <typename T>
 struct P4 {
   T x, y, z, w;
 };
-
-template <typename T>
-struct PTile {
-  P4<T> p[TILE];
-  T f[TILE * 3];
-  T n[TILE * 3];
-};
-
-template <typename T, int KT>
-__device__ __forceinline__ void accumulate_ptile(const PTile<T>& t, int cnt, int j0, int jstep, T px, T py, T pz,
-                                                 T* acc, const KConst<T>& kc) {
-  constexpr int SD = KTraits<KT>::SD;
-  constexpr bool DL = KTraits<KT>::DL;
-  const int rounds = j0 < cnt ? (cnt - j0 + jstep - 1) / jstep : 0;
-  if constexpr (KT == 111) {  // sum f / r, times 1/(4 pi) once
-    T s1 = T(0);
-#pragma unroll 4
-    for (int r = 0; r < rounds; r++) {
-      const P4<T> s = t.p[j0 + r * jstep];
-      const T x = px - s.x, y = py - s.y, z = pz - s.z;
-      const T r2 = x * x + y * y + z * z;
-      const T ri = (r2 >= T(1e-16)) ? rsqrt_t(r2) : T(0);
-      s1 += ri * s.w;
-    }
-    acc[0] += kc.c0 * s1;
-  } else {
-#pragma unroll 4
-    for (int r = 0; r < rounds; r++) {
-      const int j = j0 + r * jstep;
-      const P4<T> s = t.p[j];
-      T f[SD];
-      f[0] = s.w;
-#pragma unroll
-      for (int k = 1; k < SD; k++) f[k] = t.f[j * (SD - 1) + k - 1];
-      T nrm[3];
-      if constexpr (DL) {
-        nrm[0] = t.n[3 * j];
-        nrm[1] = t.n[3 * j + 1];
-        nrm[2] = t.n[3 * j + 2];
-      }
-      keval<KT, T>(px - s.x, py - s.y, pz - s.z, nrm, f, acc, kc);
-    }
-  }
-}
-
-// writes point k of the tile
-template <typename T, int SD, bool DL>
-__device__ __forceinline__ void put_point(PTile<T>& t, int k, T x, T y, T z, const T* f, const T* nrm) {
-  t.p[k] = P4<T>{x, y, z, f[0]};
-#pragma unroll
-  for (int s = 1; s < SD; s++) t.f[k * (SD - 1) + s - 1] = f[s];
-  if constexpr (DL) {
-    t.n[3 * k] = nrm[0];
-    t.n[3 * k + 1] = nrm[1];
-    t.n[3 * k + 2] = nrm[2];
-  }
-}
 
 __device__ __forceinline__ int group_size(int nt) {
   int g = ((nt + 31) / 32) * 32;
@@ -178,76 +119,6 @@ __device__ __forceinline__ void reduce_and_store(Red<T, 4>& red, const T* acc, i
 }
 
 // ---------------------------------------------------------------------------
-// Each thread owns up to S2M_R upward check points (tid, tid + 128, ...), so a
-// staged source feeds all of them; the leaf's sources are staged once per tile.
-constexpr int S2M_R = 4;  // |UC| <= 488 (np = 8) <= 4 x 128
-
-template <typename T, int KT>
-__global__ void __launch_bounds__(P2P_THREADS) k_s2m(P2PArgs<T> a, const int* work, int nwork, int rhs) {
-  constexpr int SD = KTraits<KT>::SD, TD = KTraits<KT>::TD;
-  constexpr bool DL = KTraits<KT>::DL;
-  __shared__ PTile<T> tile;
-  const int g = work[blockIdx.x];
-  const T rad = (T)a.radius[g];
-  const int nt = a.nuc;
-  const int sb = a.sbeg[g], sc = a.scnt[g];
-  T px[S2M_R], py[S2M_R], pz[S2M_R], acc[S2M_R][4];
-#pragma unroll
-  for (int r = 0; r < S2M_R; r++) {
-    const int ti = threadIdx.x + r * P2P_THREADS;
-    px[r] = py[r] = pz[r] = T(0);
-    if (ti < nt) {
-      px[r] = a.uc_unit[3 * ti] * rad;
-      py[r] = a.uc_unit[3 * ti + 1] * rad;
-      pz[r] = a.uc_unit[3 * ti + 2] * rad;
-    }
-#pragma unroll
-    for (int d = 0; d < 4; d++) acc[r][d] = T(0);
-  }
-  const T* den = a.sden + (size_t)rhs * a.ns * SD;
-  for (int c0 = 0; c0 < sc; c0 += TILE) {
-    const int cnt = min(TILE, sc - c0);
-    __syncthreads();
-    for (int j = threadIdx.x; j < cnt; j += blockDim.x) {
-      const int p = sb + c0 + j;
-      T f[SD], nrm[3] = {T(0), T(0), T(0)};
-#pragma unroll
-      for (int s = 0; s < SD; s++) f[s] = den[(size_t)p * SD + s];
-      if constexpr (DL) {
-        nrm[0] = a.snx[p];
-        nrm[1] = a.sny[p];
-        nrm[2] = a.snz[p];
-      }
-      put_point<T, SD, DL>(tile, j, a.sx[p], a.sy[p], a.sz[p], f, nrm);
-    }
-    __syncthreads();
-    for (int j = 0; j < cnt; j++) {  // one staged source, every check point of this thread
-      const P4<T> sp = tile.p[j];
-      T f[SD];
-      f[0] = sp.w;
-#pragma unroll
-      for (int k = 1; k < SD; k++) f[k] = tile.f[j * (SD - 1) + k - 1];
-      T nrm[3];
-      if constexpr (DL) {
-        nrm[0] = tile.n[3 * j];
-        nrm[1] = tile.n[3 * j + 1];
-        nrm[2] = tile.n[3 * j + 2];
-      }
-#pragma unroll
-      for (int r = 0; r < S2M_R; r++)
-        if (threadIdx.x + r * P2P_THREADS < nt) keval<KT, T>(px[r] - sp.x, py[r] - sp.y, pz[r] - sp.z, nrm, f, acc[r], a.ku);
-    }
-  }
-  T* outbase = a.supcval + (size_t)g * a.nuc * TD;
-#pragma unroll
-  for (int r = 0; r < S2M_R; r++) {
-    const int ti = threadIdx.x + r * P2P_THREADS;
-    if (ti < nt)
-#pragma unroll
-      for (int d = 0; d < TD; d++) outbase[(size_t)ti * TD + d] = acc[r][d];
-  }
-}
-
 template <typename T, int KT>
 __global__ void __launch_bounds__(P2P_THREADS) k_s2l(P2PArgs<T> a, const int* work, const int64_t* ptr,
                                                       const int* idx, int nwork, int rhs) {
@@ -289,155 +160,325 @@ __global__ void __launch_bounds__(P2P_THREADS) k_s2l(P2PArgs<T> a, const int* wo
   }
 }
 
-// Segment table of the sources a CTA stages: a run of point leaves or of
-// surface grids, flattened so that one shared-memory tile can span many
-// small segments (leaves average a dozen points at ptsmax=64, so staging one
-// leaf per barrier pair would leave the CTA mostly waiting).
-constexpr int SEGS = 64;
+// ---------------------------------------------------------------------------
+// Warp-per-leaf forms.  A warp owns one leaf, stages its sources 32 at a time
+// in a private slice of shared memory and synchronises with __syncwarp only,
+// so the other warps of the SM keep issuing while it waits on its loads.
+constexpr int WP_WARPS = 8;  // warps per CTA
 
 template <typename T>
-struct Segs {
-  int beg[SEGS];        // first sorted point (point segments) or node id (surface segments)
-  int pre[SEGS + 1];    // prefix sums of the segment sizes
-  T shx[SEGS], shy[SEGS], shz[SEGS], rad[SEGS];
-  const T* unit[SEGS];  // surface grid (surface segments)
-  const T* den[SEGS];   // surface densities (surface segments)
+struct WarpSrc {  // one staged batch of 32 sources
+  P4<T> p[32];
+  T f[32 * 3];
+  T n[32 * 3];
 };
 
-__device__ __forceinline__ int find_seg(const int* pre, int ns, int k) {
-  int lo = 0, hi = ns;  // pre[lo] <= k < pre[hi]
-  while (hi - lo > 1) {
-    int mid = (lo + hi) >> 1;
-    if (pre[mid] <= k)
-      lo = mid;
-    else
-      hi = mid;
+template <typename T>
+struct WarpSrc64 {  // one staged batch of 64 sources
+  P4<T> p[64];
+  T f[64 * 3];
+  T n[64 * 3];
+};
+
+// S2M: lane l owns upward check points l, l + 32, ... (R rounds); every
+// staged source (a broadcast load) updates all of them.
+template <typename T, int KT, int R>
+__global__ void __launch_bounds__(32 * WP_WARPS) k_s2m_warp(P2PArgs<T> a, const int* work, int nwork, int rhs) {
+  constexpr int SD = KTraits<KT>::SD, TD = KTraits<KT>::TD;
+  constexpr bool DL = KTraits<KT>::DL;
+  __shared__ WarpSrc<T> ws[WP_WARPS];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  WarpSrc<T>& w = ws[warp];
+  const T* den = a.sden + (size_t)rhs * a.ns * SD;
+  const int nt = a.nuc;
+  for (int wi = blockIdx.x * WP_WARPS + warp; wi < nwork; wi += gridDim.x * WP_WARPS) {
+    const int g = work[wi];
+    const T rad = (T)a.radius[g];
+    const int sb = a.sbeg[g], sc = a.scnt[g];
+    T px[R], py[R], pz[R], acc[R][TD];
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      const int ti = lane + 32 * r;
+      px[r] = py[r] = pz[r] = T(0);
+      if (ti < nt) {
+        px[r] = a.uc_unit[3 * ti] * rad;
+        py[r] = a.uc_unit[3 * ti + 1] * rad;
+        pz[r] = a.uc_unit[3 * ti + 2] * rad;
+      }
+#pragma unroll
+      for (int d = 0; d < TD; d++) acc[r][d] = T(0);
+    }
+    for (int c0 = 0; c0 < sc; c0 += 32) {
+      const int cnt = min(32, sc - c0);
+      __syncwarp();
+      if (lane < cnt) {
+        const int p = sb + c0 + lane;
+        T f[SD], nrm[3] = {T(0), T(0), T(0)};
+#pragma unroll
+        for (int s = 0; s < SD; s++) f[s] = den[(size_t)p * SD + s];
+        if constexpr (DL) {
+          nrm[0] = a.snx[p];
+          nrm[1] = a.sny[p];
+          nrm[2] = a.snz[p];
+        }
+        w.p[lane] = P4<T>{a.sx[p], a.sy[p], a.sz[p], f[0]};
+#pragma unroll
+        for (int s = 1; s < SD; s++) w.f[lane * (SD - 1) + s - 1] = f[s];
+        if constexpr (DL) {
+          w.n[3 * lane] = nrm[0];
+          w.n[3 * lane + 1] = nrm[1];
+          w.n[3 * lane + 2] = nrm[2];
+        }
+      }
+      __syncwarp();
+      for (int j = 0; j < cnt; j++) {
+        const P4<T> sp = w.p[j];
+        T f[SD];
+        f[0] = sp.w;
+#pragma unroll
+        for (int k = 1; k < SD; k++) f[k] = w.f[j * (SD - 1) + k - 1];
+        T nrm[3];
+        if constexpr (DL) {
+          nrm[0] = w.n[3 * j];
+          nrm[1] = w.n[3 * j + 1];
+          nrm[2] = w.n[3 * j + 2];
+        }
+#pragma unroll
+        for (int r = 0; r < R; r++)
+          if (32 * r < nt) keval<KT, T>(px[r] - sp.x, py[r] - sp.y, pz[r] - sp.z, nrm, f, acc[r], a.ku);
+      }
+    }
+    T* outbase = a.supcval + (size_t)g * nt * TD;
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      const int ti = lane + 32 * r;
+      if (ti < nt)
+#pragma unroll
+        for (int d = 0; d < TD; d++) outbase[(size_t)ti * TD + d] = acc[r][d];
+    }
   }
-  return lo;
 }
 
-template <typename T, int KT>
-__global__ void __launch_bounds__(P2P_THREADS) k_leaf(P2PArgs<T> a, const int* work, const int64_t* nptr,
-                                                       const int* nidx, const int64_t* mptr, const int* midx,
-                                                       int nwork, int rhs) {
+// Leaf pass: lane = (target slot, source split) with G = the power of two
+// >= the leaf's target count (<= 32) slots and 32 / G splits; splits are
+// summed with warp shuffles.  Sources are staged 32 at a time: point
+// sources from the leaf's near list (segments = source leaves, found by
+// bisection of the warp's prefix sums), then the W-list upward equivalent
+// surfaces and the leaf's own downward equivalent surface.
+template <typename T>
+struct WarpSegs {
+  int beg[32];
+  int pre[33];
+  T shx[32], shy[32], shz[32], rad[32];
+  const T* unit[32];
+  const T* den[32];
+};
+
+template <typename T, int KT, int NWARP>
+__global__ void __launch_bounds__(32 * NWARP) k_leaf_warp(P2PArgs<T> a, const int* work, const int64_t* nptr,
+                                                             const int* nidx, const int64_t* mptr, const int* midx,
+                                                             int nwork, int rhs) {
   constexpr int SD = KTraits<KT>::SD, TD = KTraits<KT>::TD;
   constexpr bool DL = KTraits<KT>::DL;
   constexpr int MM = KTraits<KT>::MM;
   constexpr int SDM = KTraits<MM>::SD;
-  __shared__ PTile<T> tile;
-  __shared__ Red<T, 4> red;
-  __shared__ Segs<T> seg;
-  const int w = blockIdx.x;
-  const int g = work[w];
-  const double cx = a.center[3 * g], cy = a.center[3 * g + 1], cz = a.center[3 * g + 2];
-  const T rad = (T)a.radius[g];
-  const int tb0 = a.tbeg[g], nt = a.tcnt[g];
-  // thread -> (target slot, source split): every thread of the CTA is busy
-  const int G = nt < P2P_THREADS ? (nt > 0 ? nt : 1) : P2P_THREADS;
-  const int nsplit = P2P_THREADS / G;
-  const int slot = threadIdx.x % G, sg = threadIdx.x / G;
-  const bool l2t = a.depth[g] >= 2;
-  T* outbase = a.tval + (size_t)rhs * a.nt * TD;
+  __shared__ WarpSrc64<T> ws[NWARP];
+  __shared__ WarpSegs<T> wg[NWARP];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  WarpSrc64<T>& w = ws[warp];
+  WarpSegs<T>& sgt = wg[warp];
   const T* den = a.sden + (size_t)rhs * a.ns * SD;
-  const int64_t nb = nptr[w], ne = nptr[w + 1];
-  const int64_t mb = mptr[w], me = mptr[w + 1];
+  T* outbase = a.tval + (size_t)rhs * a.nt * TD;
   const int nsurf = a.nsurf;
-  const int nsurf_segs = (int)(me - mb) + (l2t ? 1 : 0);
-  for (int tb = 0; tb < nt; tb += G) {
-    const int ti = tb + slot;
-    const bool valid = ti < nt && sg < nsplit;
-    T px = 0, py = 0, pz = 0;
-    if (valid) {
-      px = a.tx[tb0 + ti];
-      py = a.ty[tb0 + ti];
-      pz = a.tz[tb0 + ti];
-    }
-    T acc[4] = {0, 0, 0, 0};
-    // point sources: U list, direct W and X (user kernel, with normals)
-    for (int64_t c0 = nb; c0 < ne; c0 += SEGS) {
-      const int nseg = (int)min((int64_t)SEGS, ne - c0);
-      __syncthreads();
-      if (threadIdx.x < nseg) {
-        int s = nidx[c0 + threadIdx.x];
-        seg.beg[threadIdx.x] = a.sbeg[s];
-        seg.pre[threadIdx.x + 1] = a.scnt[s];
-        seg.shx[threadIdx.x] = (T)(a.center[3 * s] - cx);
-        seg.shy[threadIdx.x] = (T)(a.center[3 * s + 1] - cy);
-        seg.shz[threadIdx.x] = (T)(a.center[3 * s + 2] - cz);
+  for (int wi = blockIdx.x * NWARP + warp; wi < nwork; wi += gridDim.x * NWARP) {
+    const int g = work[wi];
+    const double cx = a.center[3 * g], cy = a.center[3 * g + 1], cz = a.center[3 * g + 2];
+    const T rad = (T)a.radius[g];
+    const int tb0 = a.tbeg[g], nt = a.tcnt[g];
+    const bool l2t = a.depth[g] >= 2;
+    const int64_t nb = nptr[wi], ne = nptr[wi + 1];
+    const int64_t mb = mptr[wi], me = mptr[wi + 1];
+    const int nsurf_segs = (int)(me - mb) + (l2t ? 1 : 0);
+    int G = 1;
+    while (G < nt && G < 32) G <<= 1;
+    const int nsplit = 32 / G, slot = lane % G, sg = lane / G;
+    for (int tb = 0; tb < nt; tb += G) {
+      const int ti = tb + slot;
+      const bool valid = ti < nt;
+      T px = 0, py = 0, pz = 0;
+      if (valid) {
+        px = a.tx[tb0 + ti];
+        py = a.ty[tb0 + ti];
+        pz = a.tz[tb0 + ti];
       }
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        seg.pre[0] = 0;
-        for (int e = 0; e < nseg; e++) seg.pre[e + 1] += seg.pre[e];
-      }
-      __syncthreads();
-      const int total = seg.pre[nseg];
-      for (int k0 = 0; k0 < total; k0 += TILE) {
-        const int cnt = min(TILE, total - k0);
-        // one thread per staged point; its source leaf by bisection of the prefix sums
-        for (int j = threadIdx.x; j < cnt; j += blockDim.x) {
-          const int k = k0 + j;
-          const int e = find_seg(seg.pre, nseg, k);
-          const int p = seg.beg[e] + (k - seg.pre[e]);
-          T f[SD], nrm[3] = {T(0), T(0), T(0)};
+      T acc[4] = {0, 0, 0, 0};
+      // point sources, up to 32 source leaves per batch
+      for (int64_t c0 = nb; c0 < ne; c0 += 32) {
+        const int nseg = (int)min((int64_t)32, ne - c0);
+        __syncwarp();
+        int cntl = 0;
+        if (lane < nseg) {
+          const int s = nidx[c0 + lane];
+          sgt.beg[lane] = a.sbeg[s];
+          cntl = a.scnt[s];
+          sgt.shx[lane] = (T)(a.center[3 * s] - cx);
+          sgt.shy[lane] = (T)(a.center[3 * s + 1] - cy);
+          sgt.shz[lane] = (T)(a.center[3 * s + 2] - cz);
+        }
+        // inclusive scan of the segment sizes
+        int incl = cntl;
 #pragma unroll
-          for (int s = 0; s < SD; s++) f[s] = den[(size_t)p * SD + s];
-          if constexpr (DL) {
-            nrm[0] = a.snx[p];
-            nrm[1] = a.sny[p];
-            nrm[2] = a.snz[p];
+        for (int o = 1; o < 32; o <<= 1) {
+          const int v = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += v;
+        }
+        sgt.pre[lane + 1] = incl;
+        if (lane == 0) sgt.pre[0] = 0;
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        __syncwarp();
+        for (int k0 = 0; k0 < total; k0 += 64) {
+          const int cnt = min(64, total - k0);
+#pragma unroll
+          for (int h = 0; h < 2; h++) {
+            const int jl = lane + 32 * h;
+            if (jl >= cnt) break;
+            const int k = k0 + jl;
+            int lo = 0, hi = nseg;  // pre[lo] <= k < pre[hi]
+            while (hi - lo > 1) {
+              const int mid = (lo + hi) >> 1;
+              if (sgt.pre[mid] <= k)
+                lo = mid;
+              else
+                hi = mid;
+            }
+            const int p = sgt.beg[lo] + (k - sgt.pre[lo]);
+            T f[SD];
+#pragma unroll
+            for (int s = 0; s < SD; s++) f[s] = den[(size_t)p * SD + s];
+            w.p[jl] = P4<T>{a.sx[p] + sgt.shx[lo], a.sy[p] + sgt.shy[lo], a.sz[p] + sgt.shz[lo], f[0]};
+#pragma unroll
+            for (int s = 1; s < SD; s++) w.f[jl * (SD - 1) + s - 1] = f[s];
+            if constexpr (DL) {
+              w.n[3 * jl] = a.snx[p];
+              w.n[3 * jl + 1] = a.sny[p];
+              w.n[3 * jl + 2] = a.snz[p];
+            }
           }
-          put_point<T, SD, DL>(tile, j, a.sx[p] + seg.shx[e], a.sy[p] + seg.shy[e], a.sz[p] + seg.shz[e], f, nrm);
-        }
-        __syncthreads();
-        if (valid) accumulate_ptile<T, KT>(tile, cnt, sg, nsplit, px, py, pz, acc, a.ku);
-        __syncthreads();
-      }
-    }
-    // surface sources: W-list upward equivalent surfaces (M2T) and the leaf's
-    // own downward equivalent surface (L2T), equivalent kernel
-    for (int c0 = 0; c0 < nsurf_segs; c0 += SEGS) {
-      const int nseg = min(SEGS, nsurf_segs - c0);
-      __syncthreads();
-      if (threadIdx.x < nseg) {
-        int e = c0 + threadIdx.x;
-        if (e < (int)(me - mb)) {
-          int s = midx[mb + e];
-          seg.shx[threadIdx.x] = (T)(a.center[3 * s] - cx);
-          seg.shy[threadIdx.x] = (T)(a.center[3 * s + 1] - cy);
-          seg.shz[threadIdx.x] = (T)(a.center[3 * s + 2] - cz);
-          seg.rad[threadIdx.x] = (T)a.radius[s];
-          seg.unit[threadIdx.x] = a.ue_unit;
-          seg.den[threadIdx.x] = a.supeden + (size_t)s * nsurf * SDM;
-        } else {
-          seg.shx[threadIdx.x] = seg.shy[threadIdx.x] = seg.shz[threadIdx.x] = T(0);
-          seg.rad[threadIdx.x] = rad;
-          seg.unit[threadIdx.x] = a.de_unit;
-          seg.den[threadIdx.x] = a.tdneden + (size_t)g * nsurf * SDM;
-        }
-      }
-      __syncthreads();
-      const int total = nseg * nsurf;
-      for (int k0 = 0; k0 < total; k0 += TILE) {
-        const int cnt = min(TILE, total - k0);
-        for (int j = threadIdx.x; j < cnt; j += blockDim.x) {
-          const int k = k0 + j;
-          const int e = k / nsurf, m = k - e * nsurf;
-          const T* u = seg.unit[e];
-          const T* sd = seg.den[e];
-          const T r = seg.rad[e];
-          T f[SDM];
+          __syncwarp();
+          if (valid) {
+            const int rounds = sg < cnt ? (cnt - sg + nsplit - 1) / nsplit : 0;
+            if constexpr (KT == 111) {  // sum f / r, times 1/(4 pi) once
+              T s1 = T(0);
+#pragma unroll 4
+              for (int r = 0; r < rounds; r++) {
+                const P4<T> s = w.p[sg + r * nsplit];
+                const T x = px - s.x, y = py - s.y, z = pz - s.z;
+                const T r2 = x * x + y * y + z * z;
+                const T ri = (r2 >= T(1e-16)) ? rsqrt_t(r2) : T(0);
+                s1 += ri * s.w;
+              }
+              acc[0] += a.ku.c0 * s1;
+            } else {
+#pragma unroll 4
+              for (int r = 0; r < rounds; r++) {
+                const int j = sg + r * nsplit;
+                const P4<T> s = w.p[j];
+                T f[SD];
+                f[0] = s.w;
 #pragma unroll
-          for (int s = 0; s < SDM; s++) f[s] = sd[(size_t)m * SDM + s];
-          put_point<T, SDM, false>(tile, j, u[3 * m] * r + seg.shx[e], u[3 * m + 1] * r + seg.shy[e],
-                                   u[3 * m + 2] * r + seg.shz[e], f, nullptr);
+                for (int k = 1; k < SD; k++) f[k] = w.f[j * (SD - 1) + k - 1];
+                T nrm[3];
+                if constexpr (DL) {
+                  nrm[0] = w.n[3 * j];
+                  nrm[1] = w.n[3 * j + 1];
+                  nrm[2] = w.n[3 * j + 2];
+                }
+                keval<KT, T>(px - s.x, py - s.y, pz - s.z, nrm, f, acc, a.ku);
+              }
+            }
+          }
+          __syncwarp();
         }
-        __syncthreads();
-        if (valid) accumulate_ptile<T, MM>(tile, cnt, sg, nsplit, px, py, pz, acc, a.km);
-        __syncthreads();
       }
+      // surface sources: W-list upward equivalent surfaces and the leaf's own
+      // downward equivalent surface, equivalent kernel
+      for (int c0 = 0; c0 < nsurf_segs; c0 += 32) {
+        const int nseg = min(32, nsurf_segs - c0);
+        __syncwarp();
+        if (lane < nseg) {
+          const int e = c0 + lane;
+          if (e < (int)(me - mb)) {
+            const int s = midx[mb + e];
+            sgt.shx[lane] = (T)(a.center[3 * s] - cx);
+            sgt.shy[lane] = (T)(a.center[3 * s + 1] - cy);
+            sgt.shz[lane] = (T)(a.center[3 * s + 2] - cz);
+            sgt.rad[lane] = (T)a.radius[s];
+            sgt.unit[lane] = a.ue_unit;
+            sgt.den[lane] = a.supeden + (size_t)s * nsurf * SDM;
+          } else {
+            sgt.shx[lane] = sgt.shy[lane] = sgt.shz[lane] = T(0);
+            sgt.rad[lane] = rad;
+            sgt.unit[lane] = a.de_unit;
+            sgt.den[lane] = a.tdneden + (size_t)g * nsurf * SDM;
+          }
+        }
+        __syncwarp();
+        const int total = nseg * nsurf;
+        for (int k0 = 0; k0 < total; k0 += 64) {
+          const int cnt = min(64, total - k0);
+#pragma unroll
+          for (int h = 0; h < 2; h++) {
+            const int jl = lane + 32 * h;
+            if (jl >= cnt) break;
+            const int k = k0 + jl;
+            const int e = k / nsurf, m = k - e * nsurf;
+            const T* u = sgt.unit[e];
+            const T* sd = sgt.den[e];
+            const T r = sgt.rad[e];
+            w.p[jl] = P4<T>{u[3 * m] * r + sgt.shx[e], u[3 * m + 1] * r + sgt.shy[e], u[3 * m + 2] * r + sgt.shz[e],
+                             sd[(size_t)m * SDM]};
+#pragma unroll
+            for (int s = 1; s < SDM; s++) w.f[jl * (SDM - 1) + s - 1] = sd[(size_t)m * SDM + s];
+          }
+          __syncwarp();
+          if (valid) {
+            const int rounds = sg < cnt ? (cnt - sg + nsplit - 1) / nsplit : 0;
+            if constexpr (MM == 111) {
+              T s1 = T(0);
+#pragma unroll 4
+              for (int r = 0; r < rounds; r++) {
+                const P4<T> s = w.p[sg + r * nsplit];
+                const T x = px - s.x, y = py - s.y, z = pz - s.z;
+                const T r2 = x * x + y * y + z * z;
+                const T ri = (r2 >= T(1e-16)) ? rsqrt_t(r2) : T(0);
+                s1 += ri * s.w;
+              }
+              acc[0] += a.km.c0 * s1;
+            } else {
+#pragma unroll 4
+              for (int r = 0; r < rounds; r++) {
+                const int j = sg + r * nsplit;
+                const P4<T> s = w.p[j];
+                T f[SDM];
+                f[0] = s.w;
+#pragma unroll
+                for (int k = 1; k < SDM; k++) f[k] = w.f[j * (SDM - 1) + k - 1];
+                T nrm[3];
+                keval<MM, T>(px - s.x, py - s.y, pz - s.z, nrm, f, acc, a.km);
+              }
+            }
+          }
+          __syncwarp();
+        }
+      }
+      // sum the splits (lanes slot, slot + G, ...)
+#pragma unroll
+      for (int d = 0; d < TD; d++)
+        for (int o = G; o < 32; o <<= 1) acc[d] += __shfl_xor_sync(0xffffffffu, acc[d], o);
+      if (valid && sg == 0)
+#pragma unroll
+        for (int d = 0; d < TD; d++) outbase[(size_t)(tb0 + ti) * TD + d] = acc[d];
     }
-    reduce_and_store<T, TD>(red, acc, G, nsplit, ti < nt, outbase + (size_t)(tb0 + ti) * TD, false);
   }
 }
 
@@ -508,13 +549,25 @@ template <typename T, int KT>
 void launch_p2p_kt(const P2PArgs<T>& a, const P2PWork& w, int which, int rhs, cudaStream_t st) {
   switch (which) {
     case P2P_S2M:
-      if (w.n) k_s2m<T, KT><<<w.n, P2P_THREADS, 0, st>>>(a, w.work, w.n, rhs);
+      if (w.n) {
+        const int grid = std::min((w.n + WP_WARPS - 1) / WP_WARPS, 148 * 32);
+        if (a.nuc <= 160)
+          k_s2m_warp<T, KT, 5><<<grid, 32 * WP_WARPS, 0, st>>>(a, w.work, w.n, rhs);
+        else if (a.nuc <= 320)
+          k_s2m_warp<T, KT, 10><<<grid, 32 * WP_WARPS, 0, st>>>(a, w.work, w.n, rhs);
+        else  // |UC| <= 488 for np <= 8
+          k_s2m_warp<T, KT, 16><<<grid, 32 * WP_WARPS, 0, st>>>(a, w.work, w.n, rhs);
+      }
       break;
     case P2P_S2L:
       if (w.n) k_s2l<T, KT><<<w.n, P2P_THREADS, 0, st>>>(a, w.work, w.ptr, w.idx, w.n, rhs);
       break;
     case P2P_LEAF:
-      if (w.n) k_leaf<T, KT><<<w.n, P2P_THREADS, 0, st>>>(a, w.work, w.ptr, w.idx, w.ptr2, w.idx2, w.n, rhs);
+      if (w.n) {
+        constexpr int nw = sizeof(T) == 4 ? 8 : 4;  // static shared memory: 64 staged sources per warp
+        const int grid = std::min((w.n + nw - 1) / nw, 148 * 32);
+        k_leaf_warp<T, KT, nw><<<grid, 32 * nw, 0, st>>>(a, w.work, w.ptr, w.idx, w.ptr2, w.idx2, w.n, rhs);
+      }
       break;
   }
 }
