@@ -39,13 +39,11 @@ constexpr int TC_M = 128;       // nodes per tile (MMA M, TMEM lanes)
 constexpr int TC_KC = 32;       // K per chunk (8 core matrices of 4 TF32)
 constexpr int TC_NMAX = 160;    // operator rows per tile (MMA N)
 constexpr int TC_HALF = TC_NMAX / 2;  // columns drained per thread
-constexpr int TC_THREADS = 256;
 constexpr int TC_TMEM_COLS = 512;     // two accumulators of up to 160 columns
 constexpr unsigned A_BYTES = TC_M * TC_KC * 4;        // 16 KB per head / tail
 constexpr unsigned B_BYTES = TC_NMAX * TC_KC * 4;     // 20 KB per head / tail
 constexpr unsigned A_STAGE = 2 * A_BYTES, B_STAGE = 2 * B_BYTES;
 constexpr int IMG_FLOATS = 2 * TC_NMAX * TC_KC;  // one operator chunk image: head + tail
-constexpr int OUT_LD = TC_NMAX + 4;               // staged output row stride (floats)
 // node tiles double-buffered, operator chunks triple-buffered: 184 KB, so one
 // CTA per SM, which owns all 512 TMEM columns
 constexpr unsigned TC_SMEM = 2 * A_STAGE + 3 * B_STAGE;
@@ -130,27 +128,46 @@ __device__ __forceinline__ void bulk_load(unsigned dst, const void* src, unsigne
                : "memory");
 }
 
-__global__ void __launch_bounds__(TC_THREADS, 1) k_node_gemm_tc(TcOperator A, const float* __restrict__ B,
-                                                               int64_t ldb, const int* __restrict__ bidx,
-                                                               float* __restrict__ C, int64_t ldc,
-                                                               const int* __restrict__ cidx, int ncol, int accumulate,
-                                                               GemmScale sc, int kper, double* __restrict__ partial,
-                                                               int* __restrict__ status) {
+// Work items are (node tile, N tile, K split); the grid is persistent (at
+// most one CTA per SM, each looping over items blockIdx.x, + gridDim.x, ...).
+// Warp-specialised: warps 0-7 stage node data (A stages, two) and drain the
+// accumulators (two), warp 8 issues the MMAs and the operator bulk copies (B
+// stages, three).  They hand over through mbarriers:
+//   afull[s]   (256 arrivals)  A stage s staged            worker -> MMA warp
+//   bfull[s]   (bytes)         operator chunk landed        copy   -> MMA warp
+//   accfull[b] (commit)        chunk's MMAs complete        MMA    -> workers
+//   accempty[b] (256 arrivals) accumulator b drained        worker -> MMA warp
+// The chunk stream runs straight across item boundaries; an item's stores
+// overlap the next item's MMAs.
+constexpr int TC_WORKERS = 256;
+constexpr int TC_ALL = TC_WORKERS + 32;
+
+__global__ void __launch_bounds__(TC_ALL, 1) k_node_gemm_tc(TcOperator A, const float* __restrict__ B, int64_t ldb,
+                                                           const int* __restrict__ bidx, float* __restrict__ C,
+                                                           int64_t ldc, const int* __restrict__ cidx, int ncol,
+                                                           int accumulate, GemmScale sc, int kper, int nitems,
+                                                           double* __restrict__ partial, int* __restrict__ status) {
   extern __shared__ __align__(1024) unsigned char smem[];
-  __shared__ __align__(8) unsigned long long bar[2];  // MMA completion, per accumulator
-  __shared__ __align__(8) unsigned long long opb[3];  // operator chunk arrival, per B stage
+  __shared__ __align__(8) unsigned long long afull[2], bfull[3], accfull[2], accempty[2];
   __shared__ unsigned tmem_base;
-  __shared__ int op_fail;
+  __shared__ int fail;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int n0 = blockIdx.y * A.ntile;
-  const int nn = min(A.ntile, A.Np - n0);  // rows of this tile (multiple of 16, <= 160)
-  const int half = nn / 2;                 // columns per draining thread (multiple of 8)
-  const int col0 = blockIdx.x * TC_M;
+  const int gx = (ncol + TC_M - 1) / TC_M, gy = A.ntiles;
   const int nkt = A.Kp / TC_KC;
-  // this CTA's K chunks (split K: blockIdx.z)
-  const int kb = blockIdx.z * kper, ke = min(nkt, kb + kper);
-  const int nk = ke - kb;
-  const float* img = A.img + ((size_t)blockIdx.y * nkt + kb) * IMG_FLOATS;
+  if ((int)blockIdx.x >= nitems) return;
+  const int my_items = (nitems - 1 - (int)blockIdx.x) / (int)gridDim.x + 1;
+  auto item_of = [&](int li, int& x, int& y, int& z) {
+    const int it = blockIdx.x + li * gridDim.x;
+    x = it % gx;
+    y = (it / gx) % gy;
+    z = it / (gx * gy);
+  };
+  int x0, y0, z0;
+  item_of(0, x0, y0, z0);
+  // every item of one launch has the same chunk count except a shorter last K
+  // split, which only split launches (one item per CTA) have
+  const int nk = min(nkt, (z0 + 1) * kper) - z0 * kper;
+  const int total = my_items * nk;
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
@@ -159,91 +176,56 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_node_gemm_tc(TcOperator A, co
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   if (tid == 0) {
-    for (int b = 0; b < 2; b++) mbar_init(smem_u32(&bar[b]), 1);
-    for (int b = 0; b < 3; b++) mbar_init(smem_u32(&opb[b]), 1);
-    op_fail = 0;
+    for (int b = 0; b < 2; b++) {
+      mbar_init(smem_u32(&afull[b]), TC_WORKERS);
+      mbar_init(smem_u32(&accfull[b]), 1);
+      mbar_init(smem_u32(&accempty[b]), TC_WORKERS);
+    }
+    for (int b = 0; b < 3; b++) mbar_init(smem_u32(&bfull[b]), 1);
+    fail = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const unsigned tmem = tmem_base;
-
-  auto a_stage = [&](int i) { return smem + (i & 1) * A_STAGE; };
-  auto b_stage = [&](int i) { return smem + 2 * A_STAGE + (i % 3) * B_STAGE; };
-  // operator chunk i (local): one bulk copy of its head + tail image
-  auto issue_op = [&](int i) {
-    if (tid == 0 && i < nk)
-      bulk_load(smem_u32(b_stage(i)), img + (size_t)i * IMG_FLOATS, IMG_FLOATS * 4, smem_u32(&opb[i % 3]));
+  auto a_stage = [&](int g) { return smem + (g & 1) * A_STAGE; };
+  auto b_stage = [&](int g) { return smem + 2 * A_STAGE + (g % 3) * B_STAGE; };
+  auto half_of = [&](int g) {
+    int x, y, z;
+    item_of(g / nk, x, y, z);
+    return min(A.ntile, A.Np - y * A.ntile) / 2;
   };
-  // node data: row (tid & 127) of the tile, column groups 4*(tid >> 7) .. +4
-  const int lrow = tid & (TC_M - 1), lq0 = (tid >> 7) * 4;
-  const int lj = col0 + lrow;
-  const float* bcol = (lj < ncol) ? B + (int64_t)bidx[lj] * ldb : nullptr;
-  auto load_chunk = [&](int i, float4* cur) {
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-      const int k = (kb + i) * TC_KC + 4 * (lq0 + q);
-      cur[q] = (bcol && i < nk && k < A.K) ? *reinterpret_cast<const float4*>(bcol + k)
-                                           : make_float4(0.f, 0.f, 0.f, 0.f);
-    }
-  };
-  // draining: TMEM lanes 32*(warp & 3) + lane, columns (warp >> 2) * half .. +half
-  const unsigned lane_addr = ((unsigned)((warp & 3) * 32) << 16) + (unsigned)((warp >> 2) * half);
-  float sum[TC_HALF];
-#pragma unroll
-  for (int i = 0; i < TC_HALF; i++) sum[i] = 0.f;
-  // a drain issues its loads in two groups of up to 40 columns, one wait per
-  // group; the empty asm statements pin every use of the loaded registers
-  // behind that wait
-  auto drain = [&](int buf) {
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const unsigned base = tmem + lane_addr + (unsigned)(buf * TC_NMAX);
-#pragma unroll
-    for (int g = 0; g < 2; g++) {
-      constexpr int GW = TC_HALF / 2;  // 40 columns
-      unsigned raw[GW];
-#pragma unroll
-      for (int c = 0; c < GW / 8; c++)
-        if (g * GW + c * 8 < half) tmem_ld8(base + g * GW + c * 8, &raw[c * 8]);
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-      for (int i = 0; i < GW; i++) {
-        if (g * GW + i < half) {
-          asm volatile("" : "+r"(raw[i]));
-          sum[g * GW + i] += __uint_as_float(raw[i]);
-        }
-      }
-    }
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  volatile int* vfail = &fail;
+  auto wait = [&](unsigned long long* bar, int parity) {
+    if (*vfail) return false;
+    if (mbar_wait_bounded(smem_u32(bar), parity)) return true;
+    *vfail = 1;
+    return false;
   };
 
-  const unsigned idesc = idesc_tf32(nn);
-  bool ok = true;
-  float4 cur0[4], cur1[4];
-  issue_op(0);
-  issue_op(1);
-  load_chunk(0, cur0);
-  load_chunk(1, cur1);
-  // one pipeline step on local chunk i, whose node data is in cur (refilled with chunk i + 2)
-  auto step = [&](int i, float4* cur) {
-    unsigned char* as = a_stage(i);
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-      float4 h, l;
-      split4(cur[q], h, l);
-      *reinterpret_cast<float4*>(as + core_off(lrow, lq0 + q)) = h;
-      *reinterpret_cast<float4*>(as + A_BYTES + core_off(lrow, lq0 + q)) = l;
-    }
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncthreads();
-    if (tid == 0) {
-      if (!mbar_wait_bounded(smem_u32(&opb[i % 3]), (i / 3) & 1)) op_fail = 1;
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const unsigned d = tmem + (unsigned)((i & 1) * TC_NMAX);
-      const unsigned ah0 = smem_u32(as), al0 = ah0 + A_BYTES;
-      const unsigned bh0 = smem_u32(b_stage(i)), bl0 = bh0 + B_BYTES;
-      if (!op_fail) {
+  if (warp == TC_WORKERS / 32) {
+    // ---- MMA warp: lane 0 issues the operator copies and the MMAs
+    if (lane == 0) {
+      auto issue_op = [&](int g) {
+        if (g >= total) return;
+        int x, y, z;
+        item_of(g / nk, x, y, z);
+        const float* img = A.img + ((size_t)y * nkt + z * kper + g % nk) * IMG_FLOATS;
+        bulk_load(smem_u32(b_stage(g)), img, IMG_FLOATS * 4, smem_u32(&bfull[g % 3]));
+      };
+      issue_op(0);
+      issue_op(1);
+      issue_op(2);
+      for (int g = 0; g < total; g++) {
+        if (!wait(&afull[g & 1], (g >> 1) & 1)) break;
+        if (!wait(&bfull[g % 3], (g / 3) & 1)) break;
+        if (g >= 2 && !wait(&accempty[g & 1], ((g - 2) >> 1) & 1)) break;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const unsigned d = tmem + (unsigned)((g & 1) * TC_NMAX);
+        const unsigned ah0 = smem_u32(a_stage(g)), al0 = ah0 + A_BYTES;
+        const unsigned bh0 = smem_u32(b_stage(g)), bl0 = bh0 + B_BYTES;
+        const unsigned idesc = idesc_tf32(2 * half_of(g));
 #pragma unroll
         for (int s = 0; s < TC_KC / 8; s++) {
           const unsigned off = s * 256;  // two core matrices along K per MMA
@@ -253,75 +235,143 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_node_gemm_tc(TcOperator A, co
           mma_tf32(d, ah, bl, idesc, 1);
           mma_tf32(d, al, bh, idesc, 1);
         }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         smem_u32(&accfull[g & 1]))
+                     : "memory");
+        // chunk g-1's MMAs complete -> its operator stage takes chunk g + 2
+        if (g >= 1) {
+          if (!wait(&accfull[(g - 1) & 1], ((g - 1) >> 1) & 1)) break;
+          issue_op(g + 2);
+        }
       }
-      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                       smem_u32(&bar[i & 1]))
-                   : "memory");
     }
-    load_chunk(i + 2, cur);  // in flight for two steps
-    if (i > 0) {
-      // chunk i-1's MMAs: their A / B stages and accumulator become free
-      const bool done = mbar_wait_bounded(smem_u32(&bar[(i - 1) & 1]), ((i - 1) >> 1) & 1);
-      if (__syncthreads_or(!done || op_fail)) return false;
-      drain((i - 1) & 1);
-    }
-    issue_op(i + 2);  // into the stage chunk i-1 used
-    return true;
-  };
-  for (int i = 0; i < nk && ok; i += 2) {
-    ok = step(i, cur0);
-    if (ok && i + 1 < nk) ok = step(i + 1, cur1);
-  }
-  if (ok && nk > 0) {
-    const bool done = mbar_wait_bounded(smem_u32(&bar[(nk - 1) & 1]), ((nk - 1) >> 1) & 1);
-    ok = !__syncthreads_or(!done || op_fail);
-    if (ok) drain((nk - 1) & 1);
-  }
-  if (ok) {
-    // stage the tile: row (warp & 3) * 32 + lane, columns of this thread's half
-    __syncthreads();  // every MMA has completed: the operand stages are free
-    float* out = reinterpret_cast<float*>(smem);
-    {
-      float* orow = out + ((warp & 3) * 32 + lane) * OUT_LD + (warp >> 2) * half;
+  } else {
+    // ---- worker warps: stage node data, drain accumulators, store
+    const int lrow = tid & (TC_M - 1), lq0 = (tid >> 7) * 4;
+    auto load_chunk = [&](int g, float4* cur) {
+      const float* bcol = nullptr;
+      int k0 = 0;
+      if (g < total) {
+        int x, y, z;
+        item_of(g / nk, x, y, z);
+        const int lj = x * TC_M + lrow;
+        if (lj < ncol) bcol = B + (int64_t)bidx[lj] * ldb;
+        k0 = (z * kper + g % nk) * TC_KC;
+      }
 #pragma unroll
-      for (int i = 0; i < TC_HALF; i += 4)
-        if (i < half) *reinterpret_cast<float4*>(orow + i) = make_float4(sum[i], sum[i + 1], sum[i + 2], sum[i + 3]);
-    }
-    __syncthreads();
-    const int nv = min(nn, A.M - n0);  // valid output rows of this N tile (multiple of 4)
-    const int nv4 = nv / 4;
-    const int rows = min(TC_M, ncol - col0);
-    if (partial) {  // split K: raw sums, scaled and added by the reduce
-      for (int e = tid; e < rows * nv; e += TC_THREADS) {
-        const int r = e / nv, c = e - r * nv;
-        partial[((size_t)blockIdx.z * ncol + col0 + r) * A.M + n0 + c] = (double)out[r * OUT_LD + c];
+      for (int q = 0; q < 4; q++) {
+        const int k = k0 + 4 * (lq0 + q);
+        cur[q] = (bcol && k < A.K) ? *reinterpret_cast<const float4*>(bcol + k) : make_float4(0.f, 0.f, 0.f, 0.f);
       }
-    } else {
-      for (int e = tid; e < rows * nv4; e += TC_THREADS) {
-        const int r = e / nv4, c = e - r * nv4;
-        const int j = col0 + r, n = n0 + 4 * c;
-        float4 o = *reinterpret_cast<const float4*>(out + r * OUT_LD + 4 * c);
-        if (sc.col_lvl) {
-          const int lvl = sc.col_lvl[j] + sc.lvl_base;
-          o.x *= pow2f(-lvl * sc.deg[(n + 0) % sc.sd]);
-          o.y *= pow2f(-lvl * sc.deg[(n + 1) % sc.sd]);
-          o.z *= pow2f(-lvl * sc.deg[(n + 2) % sc.sd]);
-          o.w *= pow2f(-lvl * sc.deg[(n + 3) % sc.sd]);
-        }
-        float4* p = reinterpret_cast<float4*>(C + (int64_t)cidx[j] * ldc + n);
-        if (accumulate) {
-          const float4 c4 = *p;
-          o.x += c4.x;
-          o.y += c4.y;
-          o.z += c4.z;
-          o.w += c4.w;
-        }
-        *p = o;
+    };
+    auto produce = [&](int g, const float4* cur) {
+      unsigned char* as = a_stage(g);
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        float4 h, l;
+        split4(cur[q], h, l);
+        *reinterpret_cast<float4*>(as + core_off(lrow, lq0 + q)) = h;
+        *reinterpret_cast<float4*>(as + A_BYTES + core_off(lrow, lq0 + q)) = l;
       }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&afull[g & 1])) : "memory");
+    };
+    float sum[TC_HALF];
+#pragma unroll
+    for (int i = 0; i < TC_HALF; i++) sum[i] = 0.f;
+    // drain chunk g's accumulator: TMEM lanes 32*(warp & 3) + lane, columns
+    // (warp >> 2) * half .. +half; groups of 16 columns, one wait per group,
+    // uses pinned behind the wait by empty asm statements
+    auto drain = [&](int g, int half) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const unsigned base =
+          tmem + ((unsigned)((warp & 3) * 32) << 16) + (unsigned)((warp >> 2) * half + (g & 1) * TC_NMAX);
+#pragma unroll
+      for (int gr = 0; gr < TC_HALF / 16; gr++) {
+        constexpr int GW = 16;
+        unsigned raw[GW];
+#pragma unroll
+        for (int c = 0; c < GW / 8; c++)
+          if (gr * GW + c * 8 < half) tmem_ld8(base + gr * GW + c * 8, &raw[c * 8]);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+        for (int i = 0; i < GW; i++) {
+          if (gr * GW + i < half) {
+            asm volatile("" : "+r"(raw[i]));
+            sum[gr * GW + i] += __uint_as_float(raw[i]);
+          }
+        }
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&accempty[g & 1])) : "memory");
+    };
+    // store item li's tile from the sums (row (warp & 3) * 32 + lane, this thread's half)
+    auto epilogue = [&](int li) {
+      int x, y, z;
+      item_of(li, x, y, z);
+      const int n0 = y * A.ntile, nn = min(A.ntile, A.Np - n0), half = nn / 2;
+      const int j = x * TC_M + (warp & 3) * 32 + lane;
+      const int nb = n0 + (warp >> 2) * half;
+      if (j < ncol && partial) {  // split K: raw sums, scaled and added by the reduce
+        double* pr = partial + ((size_t)z * ncol + j) * A.M;
+#pragma unroll
+        for (int i = 0; i < TC_HALF; i++)
+          if (i < half && nb + i < A.M) pr[nb + i] = (double)sum[i];
+      } else if (j < ncol) {
+        float* crow = C + (int64_t)cidx[j] * ldc;
+        const int lvl = sc.col_lvl ? sc.col_lvl[j] + sc.lvl_base : 0;
+        float f4[4];  // scale of output n: f4[n % sd], sd <= 4
+#pragma unroll
+        for (int d = 0; d < 4; d++) f4[d] = sc.col_lvl ? pow2f(-lvl * sc.deg[d < sc.sd ? d : 0]) : 1.0f;
+#pragma unroll
+        for (int i = 0; i < TC_HALF; i += 4) {
+          const int n = nb + i;
+          if (i >= half || n >= A.M) break;
+          float4 o = make_float4(sum[i], sum[i + 1], sum[i + 2], sum[i + 3]);
+          if (sc.col_lvl) {
+            o.x *= f4[(n + 0) % sc.sd];
+            o.y *= f4[(n + 1) % sc.sd];
+            o.z *= f4[(n + 2) % sc.sd];
+            o.w *= f4[(n + 3) % sc.sd];
+          }
+          float4* p = reinterpret_cast<float4*>(crow + n);
+          if (accumulate) {
+            const float4 c4 = *p;
+            o.x += c4.x;
+            o.y += c4.y;
+            o.z += c4.z;
+            o.w += c4.w;
+          }
+          *p = o;
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < TC_HALF; i++) sum[i] = 0.f;
+    };
+    float4 cur0[4], cur1[4];
+    load_chunk(0, cur0);
+    load_chunk(1, cur1);
+    if (total > 0) produce(0, cur0);
+    if (total > 1) produce(1, cur1);
+    load_chunk(2, cur0);
+    load_chunk(3, cur1);
+    // chunk g: wait for its MMAs, hand the freed A stage chunk g + 2 (data in
+    // cur, refilled with chunk g + 4), drain, store at an item's end
+    auto step = [&](int g, float4* cur) {
+      if (!wait(&accfull[g & 1], (g >> 1) & 1)) return false;
+      if (g + 2 < total) produce(g + 2, cur);
+      load_chunk(g + 4, cur);
+      drain(g, half_of(g));
+      if (g % nk == nk - 1) epilogue(g / nk);
+      return true;
+    };
+    for (int g = 0; g < total; g += 2) {
+      if (!step(g, cur0)) break;
+      if (g + 1 < total && !step(g + 1, cur1)) break;
     }
-  } else if (tid == 0) {
-    atomicOr(status, 2);
   }
+  __syncthreads();
+  if (*vfail && tid == 0) atomicOr(status, 2);
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0) {
@@ -386,10 +436,13 @@ int launch_node_gemm_tc(const TcOperator& A, const float* B, int64_t ldb, const 
   }
   const int kper = (nk + splits - 1) / splits;
   splits = (nk + kper - 1) / kper;
-  dim3 grid(gx, gy, splits);
+  const int nitems = gx * gy * splits;
+  // split launches: one item per CTA (the last split may be shorter);
+  // otherwise persistent, at most one CTA per SM
+  const int grid = splits > 1 ? nitems : std::min(nitems, num_sms);
   cudaFuncSetAttribute(k_node_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM);
-  k_node_gemm_tc<<<grid, TC_THREADS, TC_SMEM, st>>>(A, B, ldb, bidx, C, ldc, cidx, ncol, accumulate ? 1 : 0, sc, kper,
-                                                     splits > 1 ? ws : nullptr, status);
+  k_node_gemm_tc<<<grid, TC_ALL, TC_SMEM, st>>>(A, B, ldb, bidx, C, ldc, cidx, ncol, accumulate ? 1 : 0, sc, kper,
+                                                 nitems, splits > 1 ? ws : nullptr, status);
   if (splits > 1) launch_node_gemm_reduce_f(A.M, ncol, splits, ws, C, ldc, cidx, accumulate, sc, num_sms, st);
   return splits > 1 ? 2 : 1;
 }
