@@ -248,20 +248,36 @@ __global__ void __launch_bounds__(TC_ALL, 1) k_node_gemm_tc(TcOperator A, const 
   } else {
     // ---- worker warps: stage node data, drain accumulators, store
     const int lrow = tid & (TC_M - 1), lq0 = (tid >> 7) * 4;
+    // node column of this thread's row in item li (-1: past the last node)
+    auto item_col = [&](int li) {
+      int x, y, z;
+      item_of(li, x, y, z);
+      const int lj = x * TC_M + lrow;
+      return lj < ncol ? bidx[lj] : -1;
+    };
+    // load_chunk is called with g = 0, 1, 2, ...: the next item's node index is
+    // fetched one item ahead, so the data loads never wait on it
+    int li_cur = -1, idx_next = my_items > 0 ? item_col(0) : -1;
+    const float* bcol = nullptr;
     auto load_chunk = [&](int g, float4* cur) {
-      const float* bcol = nullptr;
       int k0 = 0;
+      bool have = false;
       if (g < total) {
+        const int li = g / nk;
+        if (li != li_cur) {
+          bcol = idx_next >= 0 ? B + (int64_t)idx_next * ldb : nullptr;
+          li_cur = li;
+          idx_next = li + 1 < my_items ? item_col(li + 1) : -1;
+        }
         int x, y, z;
-        item_of(g / nk, x, y, z);
-        const int lj = x * TC_M + lrow;
-        if (lj < ncol) bcol = B + (int64_t)bidx[lj] * ldb;
+        item_of(li, x, y, z);
         k0 = (z * kper + g % nk) * TC_KC;
+        have = bcol != nullptr;
       }
 #pragma unroll
       for (int q = 0; q < 4; q++) {
         const int k = k0 + 4 * (lq0 + q);
-        cur[q] = (bcol && k < A.K) ? *reinterpret_cast<const float4*>(bcol + k) : make_float4(0.f, 0.f, 0.f, 0.f);
+        cur[q] = (have && k < A.K) ? *reinterpret_cast<const float4*>(bcol + k) : make_float4(0.f, 0.f, 0.f, 0.f);
       }
     };
     auto produce = [&](int g, const float4* cur) {
@@ -280,15 +296,15 @@ __global__ void __launch_bounds__(TC_ALL, 1) k_node_gemm_tc(TcOperator A, const 
 #pragma unroll
     for (int i = 0; i < TC_HALF; i++) sum[i] = 0.f;
     // drain chunk g's accumulator: TMEM lanes 32*(warp & 3) + lane, columns
-    // (warp >> 2) * half .. +half; groups of 16 columns, one wait per group,
-    // uses pinned behind the wait by empty asm statements
+    // (warp >> 2) * half .. +half; two groups of up to 40 columns, one wait
+    // per group, uses pinned behind the wait by empty asm statements
     auto drain = [&](int g, int half) {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const unsigned base =
           tmem + ((unsigned)((warp & 3) * 32) << 16) + (unsigned)((warp >> 2) * half + (g & 1) * TC_NMAX);
 #pragma unroll
-      for (int gr = 0; gr < TC_HALF / 16; gr++) {
-        constexpr int GW = 16;
+      for (int gr = 0; gr < 2; gr++) {
+        constexpr int GW = TC_HALF / 2;  // 40 columns
         unsigned raw[GW];
 #pragma unroll
         for (int c = 0; c < GW / 8; c++)
@@ -348,26 +364,20 @@ __global__ void __launch_bounds__(TC_ALL, 1) k_node_gemm_tc(TcOperator A, const 
 #pragma unroll
       for (int i = 0; i < TC_HALF; i++) sum[i] = 0.f;
     };
-    float4 cur0[4], cur1[4];
-    load_chunk(0, cur0);
-    load_chunk(1, cur1);
-    if (total > 0) produce(0, cur0);
-    if (total > 1) produce(1, cur1);
-    load_chunk(2, cur0);
-    load_chunk(3, cur1);
-    // chunk g: wait for its MMAs, hand the freed A stage chunk g + 2 (data in
-    // cur, refilled with chunk g + 4), drain, store at an item's end
-    auto step = [&](int g, float4* cur) {
-      if (!wait(&accfull[g & 1], (g >> 1) & 1)) return false;
+    float4 cur[4];
+    load_chunk(0, cur);
+    if (total > 0) produce(0, cur);
+    load_chunk(1, cur);
+    if (total > 1) produce(1, cur);
+    load_chunk(2, cur);
+    // chunk g: wait for its MMAs, hand the freed A stage chunk g + 2 (its data
+    // in cur, then refilled with chunk g + 3), drain, store at an item's end
+    for (int g = 0; g < total; g++) {
+      if (!wait(&accfull[g & 1], (g >> 1) & 1)) break;
       if (g + 2 < total) produce(g + 2, cur);
-      load_chunk(g + 4, cur);
+      load_chunk(g + 3, cur);
       drain(g, half_of(g));
       if (g % nk == nk - 1) epilogue(g / nk);
-      return true;
-    };
-    for (int g = 0; g < total; g += 2) {
-      if (!step(g, cur0)) break;
-      if (g + 1 < total && !step(g + 1, cur1)) break;
     }
   }
   __syncthreads();
