@@ -105,7 +105,10 @@ struct Impl : ImplBase {
   T* khat;
   T* ktiles = nullptr;  // [td][sd][ceil(nf/32)][343][32] operator spectra for the parent-pair sweep
   T* ttiles = nullptr;  // [td][sd][ceil(nf/16)][26][27][16] Toeplitz-factored operator
-  int* h_status = nullptr;  // mapped host word: device-side wait time-outs (bit 0 sweep, bit 1 GEMM)
+  float* htc_img = nullptr;         // tensor-core Hadamard: operator images per (4 frequencies, direction)
+  unsigned* htc_dirs = nullptr;     // tensor-core Hadamard: directions present per tile of 128 parents
+  int cm_rows = 0;                  // tensor-core Hadamard: rows of the frequency-chunk-major spectra
+  int* h_status = nullptr;  // mapped host word: device-side wait time-outs (bit 0 sweep, bit 1 GEMM, bit 2 TC Hadamard)
   int* d_status = nullptr;
   List s2m, s2l, leaf, m2l, fwd;
   std::vector<List> up_non, dn_par;
@@ -207,7 +210,11 @@ struct Impl : ImplBase {
                 kt[dst] = kh[src];
                 kt[dst + 1] = kh[src + 1];
               }
-        if (E.m2l_toeplitz) {
+        if (sizeof(T) == 4 && E.m2l_tc && m2l_tc_supported(nf, sd_m, td_m)) {
+          std::vector<float> im;
+          m2l_tc_images(nf, op.m2l.data(), &im);
+          htc_img = upload(im);
+        } else if (E.m2l_toeplitz) {
           ttiles = upload(toeplitz_tables());
         } else {
           ktiles = upload(kt);
@@ -314,10 +321,14 @@ struct Impl : ImplBase {
       effval = dalloc<T>((size_t)nn * td_m * op.nfc * 2);
       // nn + 8 blocks: nodes outside every V list keep a zero spectrum, and the
       // 8 blocks from index nn on stand for an absent colleague (parent-pair form)
-      spectra = dalloc<T>((size_t)(nn + 8) * sd_m * op.nfc * 2);
-      KCHECK(cudaMemset(spectra, 0, sizeof(T) * (size_t)(nn + 8) * sd_m * op.nfc * 2));
+      // (tensor-core form: frequency-chunk major, node n at row n + 7 of
+      // cm_rows, so the zero block and every sibling group start on 8 rows)
+      if (htc_img) cm_rows = (nn + 15 + 7) / 8 * 8;
+      const size_t spec_len = std::max((size_t)(nn + 8) * sd_m, (size_t)cm_rows) * op.nfc * 2;
+      spectra = dalloc<T>(spec_len);
+      KCHECK(cudaMemset(spectra, 0, sizeof(T) * spec_len));
       counters_v = (double)idx.size();
-      if (ktiles || ttiles) build_pairs(work);
+      if (ktiles || ttiles || htc_img) build_pairs(work);
       counters_fwd = (double)fwdn.size();
       counters_inv = (double)work.size();
     }
@@ -380,6 +391,7 @@ struct Impl : ImplBase {
     geom.td = td_m;
     for (int s = 0; s < sd_m && s < 4; s++) geom.deg[s] = op.deg[s];
     geom.rootlvl = E.rootlvl;
+    geom.cm_rows = cm_rows;
     scl.sd = sd_m;
     for (int s = 0; s < sd_m && s < 4; s++) scl.deg[s] = op.deg[s];
     // GEMM flops per eval
@@ -527,6 +539,16 @@ struct Impl : ImplBase {
     pairs_coll = upload(coll);
     pairs_mask = upload(mask);
     pairs_n = (int)qlist.size();
+    if (htc_img) {  // directions present per tile of 128 target parents (an empty tile keeps one)
+      std::vector<unsigned> dirs((pairs_n + 127) / 128, 0u);
+      for (int t = 0; t < (int)dirs.size(); t++) {
+        for (int w = t * 128; w < std::min(pairs_n, t * 128 + 128); w++)
+          for (int d = 0; d < 26; d++)
+            if (coll[(size_t)w * 26 + d] != tr.nnodes) dirs[t] |= 1u << d;
+        if (!dirs[t]) dirs[t] = 1u;
+      }
+      htc_dirs = upload(dirs);
+    }
   }
 
   double counters_v = 0, counters_fwd = 0, counters_inv = 0, counters_near = 0, counters_surf = 0,
@@ -616,7 +638,12 @@ struct Impl : ImplBase {
       if (m2l.n > 0) {
         launch_m2l_forward<T>(geom, supeden, fwd.work, fwd.n, d_depth, spectra, st);
         if (prof && r == 0) KCHECK(cudaEventRecord(ev[7], st));
-        if (pairs_n > 0)
+        if (pairs_n > 0 && htc_img) {
+          launch_m2l_hadamard_tc(op.nfc, htc_img, reinterpret_cast<const float*>(spectra), cm_rows, pairs_n, pairs_chd,
+                                 pairs_coll, pairs_mask, htc_dirs, reinterpret_cast<float*>(effval), tr.nnodes,
+                                 d_status, num_sms, st);
+          KCHECK(cudaGetLastError());
+        } else if (pairs_n > 0)
           if (ttiles)
             launch_m2l_hadamard_tz<T>(op.nfc, sd_m, td_m, ttiles, spectra, pairs_n, pairs_chd, pairs_coll, pairs_mask,
                                       effval, tr.nnodes, d_status, num_sms, st);
@@ -769,19 +796,25 @@ int Engine::setup() {
     }
     tensor_cores = tc != 0;
     auto fit = opts.find("-" + prefix + "m2l_form");
-    // default: the factored form in mixed precision (as fast as the direct form
-    // with ~40 % fewer multiply-adds), the direct form in FP64 (faster there)
+    // default: in mixed precision the tensor-core form for single-dof kernels
+    // (tensor_cores on), else the factored form (as fast as the direct form
+    // with ~40 % fewer multiply-adds); the direct form in FP64 (faster there)
     m2l_toeplitz = mixed;
+    m2l_tc = mixed && tensor_cores;
     if (fit != opts.end()) {
       std::string v = fit->second;
       v.erase(0, v.find_first_not_of(" \t"));
       v = v.substr(0, v.find_first_of(" \t%"));
-      if (v == "direct")
+      if (v == "direct") {
         m2l_toeplitz = false;
-      else if (v == "toeplitz")
+        m2l_tc = false;
+      } else if (v == "toeplitz") {
         m2l_toeplitz = true;
-      else {
-        err = "m2l_form must be toeplitz or direct";
+        m2l_tc = false;
+      } else if (v == "tensor") {  // where unsupported (FP64, several dofs): the default form
+        m2l_tc = true;
+      } else {
+        err = "m2l_form must be tensor, toeplitz or direct";
         return KIFMM_ERR_OPTION;
       }
     }

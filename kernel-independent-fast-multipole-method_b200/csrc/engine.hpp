@@ -41,6 +41,7 @@ struct Engine {
   bool mixed = false;
   bool tensor_cores = true;  // mixed mode: surface contractions on tcgen05 (split TF32)
   bool m2l_toeplitz = false;  // V-list Hadamard in the 2x2x2 block-Toeplitz factored form
+  bool m2l_tc = false;        // mixed, single-dof kernels: V-list Hadamard on tcgen05 (split TF32)
   bool profiling = false;
   // state
   bool ready = false;       // device state built, eval allowed

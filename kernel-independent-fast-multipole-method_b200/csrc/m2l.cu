@@ -141,7 +141,10 @@ __global__ void __launch_bounds__(256) k_m2l_fwd_warp(M2LGeom g, const T* __rest
           r.re = fmt(-b.im, t.im, fmt(b.re, t.re, r.re));
           r.im = fmt(b.im, t.re, fmt(b.re, t.im, r.im));
         }
-        out[c] = r;
+        if (g.cm_rows)
+          reinterpret_cast<Cpx<T>*>(spectra)[spectra_cm_index(g.cm_rows, node, c)] = r;
+        else
+          out[c] = r;
       }
       __syncwarp();
     }
@@ -443,7 +446,10 @@ __global__ void __launch_bounds__(256) k_m2l_fwd_rb(M2LGeom g, const T* __restri
             re = fmt(-b[k].im, ci, fmt(b[k].re, cr, re));
             im = fmt(b[k].im, cr, fmt(b[k].re, ci, im));
           }
-          out[c] = Cpx<T>{re, im};
+          if (g.cm_rows)
+            reinterpret_cast<Cpx<T>*>(spectra)[spectra_cm_index(g.cm_rows, node, c)] = Cpx<T>{re, im};
+          else
+            out[c] = Cpx<T>{re, im};
         }
       }
       __syncwarp();

@@ -240,3 +240,34 @@ def test_toeplitz_hadamard_matches_direct_form(gpu, name, precision, tol):
         outs.append(out)
     diff = np.linalg.norm(outs[0] - outs[1]) / np.linalg.norm(outs[1])
     assert diff <= tol, diff
+
+
+@pytest.mark.parametrize("name", ["lap_s_np6_tt_style", "lap_s_np4_sphere", "lap_s_np8_plummer", "stk_s_np6_cube"])
+def test_tensor_core_hadamard_matches_toeplitz_form(gpu, name):
+    """The V-list product on the tensor cores (split-TF32 MMAs with the
+    gathered colleague spectra in TMEM) against the FP32 Toeplitz-factored
+    product: the same sums to split-TF32 accuracy (5e-6 relative), and both
+    as accurate against the reference as the mixed engine must be.  Stokes
+    (three dofs) has no tensor-core form and keeps the factored one, bit for
+    bit."""
+    d = G.load(name)
+    td = W.KERNEL_DOFS[d["kt"]][1]
+    outs = []
+    for form in ("tensor", "toeplitz"):
+        f = kifmm.FMM3d("fmm3d_")
+        f.srcpos, f.srcnor, f.trgpos = d["src"], d["nor"], d["trg"]
+        f.ctr, f.rootlvl = tuple(d["ctr"]), d["rootlvl"]
+        f.knl = kifmm.Kernel3d(d["kt"], d["coefs"])
+        o = G.options(d, "mixed")
+        o["-fmm3d_m2l_form"] = form
+        f.setup(o)
+        out = np.zeros(td * len(d["trg"]))
+        f.eval(d["den"], out)
+        err = oracle.relerr(out.reshape(-1, td)[d["chk"]], d["ref_direct"])
+        assert err <= max(10 * d["ref_relerr"], MIXED_FLOOR), (form, err, d["ref_relerr"])
+        outs.append(out)
+    diff = np.linalg.norm(outs[0] - outs[1]) / np.linalg.norm(outs[1])
+    if td == 3:
+        assert diff == 0.0, diff
+    else:
+        assert diff <= 5e-6, diff
