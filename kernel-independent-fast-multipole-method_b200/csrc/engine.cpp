@@ -107,7 +107,6 @@ struct Impl : ImplBase {
   T* ttiles = nullptr;  // [td][sd][ceil(nf/16)][26][27][16] Toeplitz-factored operator
   float* htc_img = nullptr;         // tensor-core Hadamard: operator images per (4 frequencies, direction)
   unsigned* htc_dirs = nullptr;     // tensor-core Hadamard: directions present per tile of 128 parents
-  int cm_rows = 0;                  // tensor-core Hadamard: rows of the frequency-chunk-major spectra
   int* h_status = nullptr;  // mapped host word: device-side wait time-outs (bit 0 sweep, bit 1 GEMM, bit 2 TC Hadamard)
   int* d_status = nullptr;
   List s2m, s2l, leaf, m2l, fwd;
@@ -321,10 +320,9 @@ struct Impl : ImplBase {
       effval = dalloc<T>((size_t)nn * td_m * op.nfc * 2);
       // nn + 8 blocks: nodes outside every V list keep a zero spectrum, and the
       // 8 blocks from index nn on stand for an absent colleague (parent-pair form)
-      // (tensor-core form: frequency-chunk major, node n at row n + 7 of
-      // cm_rows, so the zero block and every sibling group start on 8 rows)
-      if (htc_img) cm_rows = (nn + 15 + 7) / 8 * 8;
-      const size_t spec_len = std::max((size_t)(nn + 8) * sd_m, (size_t)cm_rows) * op.nfc * 2;
+      // (tensor-core form: sibling-group major, node n in group (n + 7) / 8,
+      // the zero block a group of its own: (nn + 15) / 8 groups of 8 nodes)
+      const size_t spec_len = std::max((size_t)(nn + 8) * sd_m, htc_img ? (size_t)(nn + 15) / 8 * 8 : 0) * op.nfc * 2;
       spectra = dalloc<T>(spec_len);
       KCHECK(cudaMemset(spectra, 0, sizeof(T) * spec_len));
       counters_v = (double)idx.size();
@@ -391,7 +389,7 @@ struct Impl : ImplBase {
     geom.td = td_m;
     for (int s = 0; s < sd_m && s < 4; s++) geom.deg[s] = op.deg[s];
     geom.rootlvl = E.rootlvl;
-    geom.cm_rows = cm_rows;
+    geom.sg = htc_img ? 1 : 0;
     scl.sd = sd_m;
     for (int s = 0; s < sd_m && s < 4; s++) scl.deg[s] = op.deg[s];
     // GEMM flops per eval
@@ -639,7 +637,7 @@ struct Impl : ImplBase {
         launch_m2l_forward<T>(geom, supeden, fwd.work, fwd.n, d_depth, spectra, st);
         if (prof && r == 0) KCHECK(cudaEventRecord(ev[7], st));
         if (pairs_n > 0 && htc_img) {
-          launch_m2l_hadamard_tc(op.nfc, htc_img, reinterpret_cast<const float*>(spectra), cm_rows, pairs_n, pairs_chd,
+          launch_m2l_hadamard_tc(op.nfc, htc_img, reinterpret_cast<const float*>(spectra), pairs_n, pairs_chd,
                                  pairs_coll, pairs_mask, htc_dirs, reinterpret_cast<float*>(effval), tr.nnodes,
                                  d_status, num_sms, st);
           KCHECK(cudaGetLastError());

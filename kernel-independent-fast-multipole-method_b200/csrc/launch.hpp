@@ -113,14 +113,16 @@ struct M2LGeom {
   int sd = 1, td = 1;
   int deg[4] = {0, 0, 0, 0};
   int rootlvl = 0;
-  // 0: spectra[node][s][f]; > 0 (single dof): frequency-chunk major,
-  // spectra[f / 4][node + 7][f % 4] over cm_rows rows (a multiple of 8, so
-  // every sibling group of 8 starts on a 256-byte boundary)
-  int cm_rows = 0;
+  // 0: spectra[node][s][f]; 1 (single dof): sibling-group major,
+  // spectra[(node + 7) / 8][f / 4][(node + 7) % 8][f % 4] -- every sibling
+  // group's spectra one block, and in it the 8 children's values of 4
+  // frequencies 256 contiguous bytes (first children are 1 mod 8)
+  int sg = 0;
 };
-// complex index of (node, compact frequency c) in the frequency-chunk-major layout
-__host__ __device__ inline size_t spectra_cm_index(int cm_rows, int node, int c) {
-  return ((size_t)(c >> 2) * cm_rows + node + 7) * 4 + (c & 3);
+// complex index of (node, compact frequency c) in the sibling-group-major
+// layout of nfc frequencies (a multiple of 4)
+__host__ __device__ inline size_t spectra_sg_index(int nfc, int node, int c) {
+  return (((size_t)((node + 7) >> 3) * (nfc >> 2) + (c >> 2)) * 8 + ((node + 7) & 7)) * 4 + (c & 3);
 }
 
 // spectra[node][s][f] (complex, interleaved re/im) of 2^(l*deg) * supeden[node]
@@ -155,13 +157,13 @@ void launch_m2l_hadamard_tz(int nf, int sd, int td, const T* ttiles, const T* sp
 // The same product for single-dof kernels in FP32 on the tensor cores
 // (m2l_tc.cu): tiles of 128 target parents, per frequency a split-TF32 MMA
 // with the gathered colleague spectra in TMEM; spectra in the
-// frequency-chunk-major layout of cm_rows rows.  img: per (chunk of 4
+// sibling-group-major layout.  img: per (chunk of 4
 // frequencies, direction) the head and tail images of the 16 x 16 real
 // blocks (m2l_tc_images); tile_dirs[t]: the directions present among tile
 // t's parents (bit d; never 0).  A wait that times out sets bit 2 of *status.
 bool m2l_tc_supported(int nf, int sd, int td);
 void m2l_tc_images(int nf, const std::complex<double>* m2l, std::vector<float>* img);
-void launch_m2l_hadamard_tc(int nf, const float* img, const float* spectra, int cm_rows, int nq, const int* qchd,
+void launch_m2l_hadamard_tc(int nf, const float* img, const float* spectra, int nq, const int* qchd,
                             const int* coll, const unsigned char* mask, const unsigned* tile_dirs, float* effval,
                             int zero_node, int* status, int num_sms, cudaStream_t st);
 // tdncval[node] += extract(inverse(effval[node]))

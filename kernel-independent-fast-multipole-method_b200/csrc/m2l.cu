@@ -141,8 +141,8 @@ __global__ void __launch_bounds__(256) k_m2l_fwd_warp(M2LGeom g, const T* __rest
           r.re = fmt(-b.im, t.im, fmt(b.re, t.re, r.re));
           r.im = fmt(b.im, t.re, fmt(b.re, t.im, r.im));
         }
-        if (g.cm_rows)
-          reinterpret_cast<Cpx<T>*>(spectra)[spectra_cm_index(g.cm_rows, node, c)] = r;
+        if (g.sg)
+          reinterpret_cast<Cpx<T>*>(spectra)[spectra_sg_index(nfc, node, c)] = r;
         else
           out[c] = r;
       }
@@ -446,8 +446,8 @@ __global__ void __launch_bounds__(256) k_m2l_fwd_rb(M2LGeom g, const T* __restri
             re = fmt(-b[k].im, ci, fmt(b[k].re, cr, re));
             im = fmt(b[k].im, cr, fmt(b[k].re, ci, im));
           }
-          if (g.cm_rows)
-            reinterpret_cast<Cpx<T>*>(spectra)[spectra_cm_index(g.cm_rows, node, c)] = Cpx<T>{re, im};
+          if (g.sg)
+            reinterpret_cast<Cpx<T>*>(spectra)[spectra_sg_index(NFC, node, c)] = Cpx<T>{re, im};
           else
             out[c] = Cpx<T>{re, im};
         }

@@ -19,9 +19,9 @@
 // values, split them into a TF32 head and tail and write both into TMEM with
 // tcgen05.st, where the MMA reads A directly (an MMA with A in shared memory
 // at N = 16 is bound by the shared-memory reads of A, one with A in TMEM by
-// the tensor core).  The spectra are stored frequency-chunk major
-// ([f / 4][node + 7][f % 4], written so by the forward transform), so a
-// colleague's 8 children x 4 frequencies are 256 contiguous bytes; four
+// the tensor core).  The spectra are stored sibling-group major (written so
+// by the forward transform), so a colleague's 8 children x 4 frequencies
+// are 256 contiguous bytes; four
 // adjacent threads load children 4 kh .. 4 kh + 3 of one row with 32-byte
 // loads (one 128-byte line per row per load instruction) and write them with
 // the 16x256b TMEM shape, whose four adjacent threads fill one lane's 8
@@ -44,14 +44,15 @@
 //               match the parity of a phase two behind); the group also
 //               issues the step's operator copy (operator stage s mod 6) and
 //               arrives on afull only once it has landed
-//   warp 12     MMA warp: per step one wait, 16 MMAs (one elected lane), one
-//               commit; at an item's end it also drains TMEM lane quarter 0
-//   warps 13-15 drain lane quarters 1-3: accumulator -> registers -> effval
+//   warps 12-15 MMA warps: warp 12 + f issues frequency f's 4 MMAs of every
+//               step (its own accumulator columns; one elected lane) and
+//               commits; at an item's end it drains TMEM lane quarter
+//               (12 + f) mod 4, all four frequencies, into effval
 //   bfull[6]   (bytes)         operator images landed           copy -> producers
 //   afull[3]   (128 arrivals)  A stage written, images landed   producers -> MMA
-//   aempty[3]  (commit)        step's MMAs done: A stage and the operator
+//   aempty[3]  (4 commits)     step's MMAs done: A stage and the operator
 //                              stage of step - 3 free           MMA -> producers
-//   accfull    (commit)        item's MMAs done                 MMA -> drain
+//   accfull    (4 commits)     item's MMAs done                 MMA -> drain
 //   accempty   (128 arrivals)  accumulator read out             drain -> MMA
 // Every wait is bounded; a time-out sets bit 2 of *status and ends the CTA.
 #include <algorithm>
@@ -114,66 +115,32 @@ __device__ __forceinline__ constexpr unsigned idesc_tf32() {
   return (1u << 4) | (2u << 7) | (2u << 10) | ((unsigned)(N >> 3) << 17) | ((unsigned)(HT_M >> 4) << 24);
 }
 
-// one step's 16 MMAs in one block, issued by one elected lane of the
-// converged warp: for frequency f and K-half kh (A columns a0 + 32 f + 8 kh
-// head, + 16 tail; operator block b0 + 2048 f + 1024 kh bytes)
-//   D[d0 + 32 f, +32) (+)= A_hi [B_hi | B_lo]^T,  D[d0 + 32 f, +16) += A_lo B_hi^T
-// the first product of each frequency overwrites D when acc == 0
-__device__ __forceinline__ void mma_step(unsigned d0, unsigned a0, uint64_t b0, int acc) {
+// one frequency's 4 MMAs of a step in one block, issued by one elected
+// lane of the converged warp: for K-half kh (A columns a + 8 kh head, + 16
+// tail; operator block at descriptor b + 1024 kh bytes)
+//   D[d, +32) (+)= A_hi [B_hi | B_lo]^T,  D[d, +16) += A_lo B_hi^T
+// the first product overwrites D when acc == 0
+__device__ __forceinline__ void mma_freq(unsigned d, unsigned a, uint64_t b, int acc) {
   asm volatile(
       "{\n"
       " .reg .pred e, p, t;\n"
-      " .reg .b32 d, a;\n"
+      " .reg .b32 a;\n"
       " .reg .b64 b;\n"
       " setp.ne.b32 p, %3, 0;\n"
       " setp.eq.b32 t, %3, %3;\n"
       " elect.sync _|e, 0xffffffff;\n"
-      " add.u32 d, %0, 0;\n"
       " add.u64 b, %2, 0;\n"
       " add.u32 a, %1, 0;\n"
-      " @e tcgen05.mma.cta_group::1.kind::tf32 [d], [a], b, %4, p;\n"
+      " @e tcgen05.mma.cta_group::1.kind::tf32 [%0], [a], b, %4, p;\n"
       " add.u32 a, %1, 16;\n"
-      " @e tcgen05.mma.cta_group::1.kind::tf32 [d], [a], b, %5, t;\n"
+      " @e tcgen05.mma.cta_group::1.kind::tf32 [%0], [a], b, %5, t;\n"
       " add.u64 b, %2, 64;\n"
       " add.u32 a, %1, 8;\n"
-      " @e tcgen05.mma.cta_group::1.kind::tf32 [d], [a], b, %4, t;\n"
+      " @e tcgen05.mma.cta_group::1.kind::tf32 [%0], [a], b, %4, t;\n"
       " add.u32 a, %1, 24;\n"
-      " @e tcgen05.mma.cta_group::1.kind::tf32 [d], [a], b, %5, t;\n"
-      " add.u32 d, %0, 32;\n"
-      " add.u64 b, %2, 128;\n"
-      " add.u32 a, %1, 32;\n"
-      " @e tcgen05.mma.cta_group::1.kind::tf32 [d], [a], b, %4, p;\n"
-      " add.u32 a, %1, 48;\n"
-      " @e tcgen05.mma.cta_group::1.kind::tf32 [d], [a], b, %5, t;\n"
-      " add.u64 b, %2, 192;\n"
-      " add.u32 a, %1, 40;\n"
-      " @e tcgen05.mma.cta_group::1.kind::tf32 [d], [a], b, %4, t;\n"
-      " add.u32 a, %1, 56;\n"
-      " @e tcgen05.mma.cta_group::1.kind::tf32 [d], [a], b, %5, t;\n"
-      " add.u32 d, %0, 64;\n"
-      " add.u64 b, %2, 256;\n"
-      " add.u32 a, %1, 64;\n"
-      " @e tcgen05.mma.cta_group::1.kind::tf32 [d], [a], b, %4, p;\n"
-      " add.u32 a, %1, 80;\n"
-      " @e tcgen05.mma.cta_group::1.kind::tf32 [d], [a], b, %5, t;\n"
-      " add.u64 b, %2, 320;\n"
-      " add.u32 a, %1, 72;\n"
-      " @e tcgen05.mma.cta_group::1.kind::tf32 [d], [a], b, %4, t;\n"
-      " add.u32 a, %1, 88;\n"
-      " @e tcgen05.mma.cta_group::1.kind::tf32 [d], [a], b, %5, t;\n"
-      " add.u32 d, %0, 96;\n"
-      " add.u64 b, %2, 384;\n"
-      " add.u32 a, %1, 96;\n"
-      " @e tcgen05.mma.cta_group::1.kind::tf32 [d], [a], b, %4, p;\n"
-      " add.u32 a, %1, 112;\n"
-      " @e tcgen05.mma.cta_group::1.kind::tf32 [d], [a], b, %5, t;\n"
-      " add.u64 b, %2, 448;\n"
-      " add.u32 a, %1, 104;\n"
-      " @e tcgen05.mma.cta_group::1.kind::tf32 [d], [a], b, %4, t;\n"
-      " add.u32 a, %1, 120;\n"
-      " @e tcgen05.mma.cta_group::1.kind::tf32 [d], [a], b, %5, t;\n"
-      "}\n" ::"r"(d0),
-      "r"(a0), "l"(b0), "r"(acc), "r"(idesc_tf32<32>()), "r"(idesc_tf32<16>())
+      " @e tcgen05.mma.cta_group::1.kind::tf32 [%0], [a], b, %5, t;\n"
+      "}\n" ::"r"(d),
+      "r"(a), "l"(b), "r"(acc), "r"(idesc_tf32<32>()), "r"(idesc_tf32<16>())
       : "memory");
 }
 
@@ -225,11 +192,14 @@ __device__ __forceinline__ void tmem_ld32(unsigned taddr, unsigned* r) {
       : "r"(taddr));
 }
 
-// TF32 head (round to nearest) and the exact FP32 remainder; the tensor core
-// reads the remainder's leading 10 mantissa bits
-__device__ __forceinline__ void split_hl(float x, unsigned& hi, unsigned& lo) {
-  hi = (__float_as_uint(x) + 0x1000u) & 0xFFFFE000u;
-  lo = __float_as_uint(x - __uint_as_float(hi));
+// TF32 heads (the leading 10 mantissa bits) of a complex value and the exact
+// FP32 remainders; the tensor core reads the remainders' leading 10 mantissa
+// bits (relative error of a split value below 2^-20)
+__device__ __forceinline__ void split_hl2(float re, float im, unsigned* hi, unsigned* lo) {
+  hi[0] = __float_as_uint(re) & 0xFFFFE000u;
+  hi[1] = __float_as_uint(im) & 0xFFFFE000u;
+  lo[0] = __float_as_uint(re - __uint_as_float(hi[0]));
+  lo[1] = __float_as_uint(im - __uint_as_float(hi[1]));
 }
 
 // The step sequence of one CTA: (item, direction) over its items in order,
@@ -241,7 +211,7 @@ struct StepIter {
 
 template <int NF>
 __global__ void __launch_bounds__(HT_THREADS, 1)
-    k_m2l_had_tc(const float* __restrict__ img, const float* __restrict__ spectra, int cm_rows, int nq, int ntiles,
+    k_m2l_had_tc(const float* __restrict__ img, const float* __restrict__ spectra, int nq, int ntiles,
                  const int* __restrict__ qchd, const int* __restrict__ coll, const unsigned char* __restrict__ mask,
                  const unsigned* __restrict__ tile_dirs, float* __restrict__ effval, int zero_node, int nitems,
                  int* __restrict__ status) {
@@ -263,12 +233,12 @@ __global__ void __launch_bounds__(HT_THREADS, 1)
   if (tid == 0) {
     for (int b = 0; b < HT_ASTAGES; b++) {
       mbar_init(smem_u32(&afull[b]), 128);
-      mbar_init(smem_u32(&aempty[b]), 1);
+      mbar_init(smem_u32(&aempty[b]), HT_F);
     }
     for (int b = 0; b < HT_NB; b++) mbar_init(smem_u32(&bfull[b]), 1);
-    mbar_init(smem_u32(&accfull), 1);
+    mbar_init(smem_u32(&accfull), HT_F);
     mbar_init(smem_u32(&accempty), 128);
-    mbar_init(smem_u32(&lastbar), 1);
+    mbar_init(smem_u32(&lastbar), HT_F);
     fail = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -356,12 +326,30 @@ __global__ void __launch_bounds__(HT_THREADS, 1)
     // + 31 in two halves of 16; thread t carries rows t / 4 and t / 4 + 8 of
     // each half and child 4 kh + t % 4 of each row's colleague
     const int grp = warp >> 2, qd = warp & 3, c = lane & 3;
+    // colleague first children of this thread's rows 32 qd + 16 h + 8 ab + t / 4
+    auto load_nb = [&](const StepIter& x, int* nb) {
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        const int q = x.tile * HT_M + qd * 32 + 16 * (k >> 1) + 8 * (k & 1) + (lane >> 2);
+        nb[k] = q < nq ? __ldg(coll + (size_t)q * 26 + x.d) : zero_node;
+      }
+    };
     StepIter it;
     start(it, 0);
     int s = 0, pend = -1;  // pend: step of an operator copy not yet seen landed
+    int nb[4];             // colleague indices of this group's next step, fetched a step early
+    bool have_nb = false;
     while (next(it)) {
       const int stg = s % HT_ASTAGES;
-      if (stg == grp) {
+      if (stg != grp) {
+        if ((s + 1) % HT_ASTAGES == grp) {  // the next step is this group's
+          StepIter nx = it;
+          have_nb = next(nx);
+          if (have_nb) load_nb(nx, nb);
+        }
+      } else {
+        if (!have_nb) load_nb(it, nb);
+        have_nb = false;
         // the step's operator images into stage s mod 6, last read by step
         // s - 6, whose MMAs completed before this group's stage wait of step
         // s - 3 (stages s mod 6 and s + 3 mod 6 belong to this group alone)
@@ -373,14 +361,12 @@ __global__ void __launch_bounds__(HT_THREADS, 1)
         // v[h][ab][kh]: 4 complex (frequencies f0 .. f0 + 3) of child 4 kh + c
         // of the colleague of row 32 qd + 16 h + 8 ab + t / 4
         float v[2][2][2][8];
-        const float* chunk = spectra + (size_t)it.fc * cm_rows * 8;
 #pragma unroll
         for (int h = 0; h < 2; h++)
 #pragma unroll
           for (int ab = 0; ab < 2; ab++) {
-            const int q = it.tile * HT_M + qd * 32 + 16 * h + 8 * ab + (lane >> 2);
-            const int nb = q < nq ? __ldg(coll + (size_t)q * 26 + it.d) : zero_node;
-            const float* row = chunk + (size_t)(nb + 7 + c) * 8;
+            // the colleague's block of this chunk: 8 children x 4 frequencies
+            const float* row = spectra + (((size_t)((nb[2 * h + ab] + 7) >> 3) * (NF / HT_F) + it.fc) * 8 + c) * 8;
             ld32B(row, v[h][ab][0]);
             ld32B(row + 32, v[h][ab][1]);
           }
@@ -397,10 +383,8 @@ __global__ void __launch_bounds__(HT_THREADS, 1)
 #pragma unroll
             for (int kh = 0; kh < 2; kh++)
 #pragma unroll
-              for (int ab = 0; ab < 2; ab++) {
-                split_hl(v[h][ab][kh][2 * f], r[4 * kh + 2 * ab], r[8 + 4 * kh + 2 * ab]);
-                split_hl(v[h][ab][kh][2 * f + 1], r[4 * kh + 2 * ab + 1], r[8 + 4 * kh + 2 * ab + 1]);
-              }
+              for (int ab = 0; ab < 2; ab++)
+                split_hl2(v[h][ab][kh][2 * f], v[h][ab][kh][2 * f + 1], &r[4 * kh + 2 * ab], &r[8 + 4 * kh + 2 * ab]);
             tmem_st16x256_x4(abase + ((unsigned)(qd * 32 + 16 * h) << 16) + f * 32, r);
           }
         asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
@@ -415,13 +399,15 @@ __global__ void __launch_bounds__(HT_THREADS, 1)
     }
     // after a time-out: the copy this warp issued last has landed before the CTA ends
     if (pend >= 0) mbar_wait_bounded(smem_u32(&bfull[pend % HT_NB]), (pend / HT_NB) & 1);
-  } else if (warp == HT_MMA_WARP) {
-    // ---- MMA warp.  The next step's afull is tested (without blocking)
-    // before this step's MMAs go out, so the test's latency hides behind them
+  } else {
+    // ---- MMA warps: warp HT_MMA_WARP + f, frequency f.  The next step's
+    // afull is tested (without blocking) before this step's MMAs go out, so
+    // the test's latency hides behind them
+    const int f = warp - HT_MMA_WARP;
     StepIter it;
     start(it, 0);
     int s = 0;
-    bool first = true;  // first step of an item
+    bool first = true;   // first step of an item
     bool ready = false;  // afull of step s seen complete
     while (next(it)) {
       const int stg = s % HT_ASTAGES;
@@ -430,24 +416,20 @@ __global__ void __launch_bounds__(HT_THREADS, 1)
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const int s1 = s + 1;
       ready = mbar_test(smem_u32(&afull[s1 % HT_ASTAGES]), (s1 / HT_ASTAGES) & 1);
-      mma_step(tmem, tmem + HT_ACOL0 + (unsigned)stg * (HT_F * 32),
-               img_desc(smem_u32(smem + (size_t)(s % HT_NB) * HT_IMG_BYTES)), first ? 0 : 1);
+      mma_freq(tmem + f * 32, tmem + HT_ACOL0 + (unsigned)stg * (HT_F * 32) + f * 32,
+               img_desc(smem_u32(smem + (size_t)(s % HT_NB) * HT_IMG_BYTES + f * 2048)), first ? 0 : 1);
       commit_elect(smem_u32(&aempty[stg]));
       first = last_of_item(it);
       s++;
       if (first) {
         commit_elect(smem_u32(&accfull));
-        if (!drain(it.li)) break;  // lane quarter 0 of the item just finished
+        if (!drain(it.li)) break;  // lane quarter warp mod 4 of the item just finished
       }
     }
     // before the CTA ends every MMA issued has completed (only a time-out
     // leaves any outstanding)
     commit_elect(smem_u32(&lastbar));
     mbar_wait_bounded(smem_u32(&lastbar), 0);
-  } else {
-    // ---- drain warps: lane quarters 1-3
-    for (int li = 0; li < my_items; li++)
-      if (!drain(li)) break;
   }
   __syncthreads();
   if (*vfail && tid == 0) atomicOr(status, 4);
@@ -460,7 +442,7 @@ __global__ void __launch_bounds__(HT_THREADS, 1)
 }
 
 template <int NF>
-void had_tc_launch(const float* img, const float* spectra, int cm_rows, int nq, const int* qchd, const int* coll,
+void had_tc_launch(const float* img, const float* spectra, int nq, const int* qchd, const int* coll,
                    const unsigned char* mask, const unsigned* tile_dirs, float* effval, int zero_node, int* status,
                    int num_sms, cudaStream_t st) {
   const int ntiles = (nq + HT_M - 1) / HT_M;
@@ -470,8 +452,8 @@ void had_tc_launch(const float* img, const float* spectra, int cm_rows, int nq, 
   auto kern = k_m2l_had_tc<NF>;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   const int grid = std::min(num_sms, nitems);
-  kern<<<grid, HT_THREADS, smem, st>>>(img, spectra, cm_rows, nq, ntiles, qchd, coll, mask, tile_dirs, effval,
-                                       zero_node, nitems, status);
+  kern<<<grid, HT_THREADS, smem, st>>>(img, spectra, nq, ntiles, qchd, coll, mask, tile_dirs, effval, zero_node,
+                                       nitems, status);
 }
 
 inline float tf32_round_host(float x) {
@@ -521,15 +503,15 @@ void m2l_tc_images(int nf, const std::complex<double>* m2l, std::vector<float>* 
   }
 }
 
-void launch_m2l_hadamard_tc(int nf, const float* img, const float* spectra, int cm_rows, int nq, const int* qchd,
+void launch_m2l_hadamard_tc(int nf, const float* img, const float* spectra, int nq, const int* qchd,
                             const int* coll, const unsigned char* mask, const unsigned* tile_dirs, float* effval,
                             int zero_node, int* status, int num_sms, cudaStream_t st) {
   if (nf == 868)
-    had_tc_launch<868>(img, spectra, cm_rows, nq, qchd, coll, mask, tile_dirs, effval, zero_node, status, num_sms, st);
+    had_tc_launch<868>(img, spectra, nq, qchd, coll, mask, tile_dirs, effval, zero_node, status, num_sms, st);
   else if (nf == 260)
-    had_tc_launch<260>(img, spectra, cm_rows, nq, qchd, coll, mask, tile_dirs, effval, zero_node, status, num_sms, st);
+    had_tc_launch<260>(img, spectra, nq, qchd, coll, mask, tile_dirs, effval, zero_node, status, num_sms, st);
   else if (nf == 2052)
-    had_tc_launch<2052>(img, spectra, cm_rows, nq, qchd, coll, mask, tile_dirs, effval, zero_node, status, num_sms,
+    had_tc_launch<2052>(img, spectra, nq, qchd, coll, mask, tile_dirs, effval, zero_node, status, num_sms,
                         st);
 }
 
