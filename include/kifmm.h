@@ -161,7 +161,8 @@ kifmm_status kifmm_set_profiling(kifmm_handle h, int on);
  * [0] U-list point-point interactions, [1] V-list node pairs,
  * [2] W/X direct interactions, [3] nodes, [4] leaves, [5] surface GEMM flops
  * per eval, [6] forward spectra per eval, [7] inverse spectra per eval,
- * [8] S2M + L2T + M2T + S2L point-surface interactions. */
+ * [8] S2M + L2T + M2T + S2L point-surface interactions, [9] tensor-core flops
+ * per eval of the V-list Hadamard (0 unless that form is used). */
 kifmm_status kifmm_work_counters(kifmm_handle h, double* counts, int* n);
 
 /* Number of this library's kernel launches issued by the last eval. */

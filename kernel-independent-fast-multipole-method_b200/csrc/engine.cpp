@@ -539,18 +539,23 @@ struct Impl : ImplBase {
     pairs_n = (int)qlist.size();
     if (htc_img) {  // directions present per tile of 128 target parents (an empty tile keeps one)
       std::vector<unsigned> dirs((pairs_n + 127) / 128, 0u);
+      double steps = 0;
       for (int t = 0; t < (int)dirs.size(); t++) {
         for (int w = t * 128; w < std::min(pairs_n, t * 128 + 128); w++)
           for (int d = 0; d < 26; d++)
             if (coll[(size_t)w * 26 + d] != tr.nnodes) dirs[t] |= 1u << d;
         if (!dirs[t]) dirs[t] = 1u;
+        steps += __builtin_popcount(dirs[t]);
       }
+      // executed MMA work: per (tile, direction, 4 frequencies) 8 MMAs of
+      // 128 x 32 x 8 and 8 of 128 x 16 x 8
+      counters_tc_had = steps * (op.nfc / 4) * (8.0 * 2 * 128 * 32 * 8 + 8.0 * 2 * 128 * 16 * 8);
       htc_dirs = upload(dirs);
     }
   }
 
   double counters_v = 0, counters_fwd = 0, counters_inv = 0, counters_near = 0, counters_surf = 0,
-         counters_gemm = 0;
+         counters_gemm = 0, counters_tc_had = 0;
 
   List make_list(const std::vector<int>& work, const std::vector<int>& aux, const std::vector<int64_t>& ptr = {},
                  const std::vector<int>& idx = {}, const std::vector<int64_t>& ptr2 = {},
@@ -851,13 +856,13 @@ int Engine::setup() {
       auto p = std::make_unique<Impl<float>>(*this);
       p->build();
       counters = {p->counters_near, p->counters_v, 0, (double)tree.nnodes, 0, p->counters_gemm, p->counters_fwd,
-                  p->counters_inv, p->counters_surf};
+                  p->counters_inv, p->counters_surf, p->counters_tc_had};
       impl = std::move(p);
     } else {
       auto p = std::make_unique<Impl<double>>(*this);
       p->build();
       counters = {p->counters_near, p->counters_v, 0, (double)tree.nnodes, 0, p->counters_gemm, p->counters_fwd,
-                  p->counters_inv, p->counters_surf};
+                  p->counters_inv, p->counters_surf, p->counters_tc_had};
       impl = std::move(p);
     }
     int nleaf = 0;

@@ -264,7 +264,7 @@ class FMM3d:
         n = ctypes.c_int()
         self._check(lib().kifmm_work_counters(self._h, c, ctypes.byref(n)))
         names = ("near_interactions", "v_pairs", "wx_direct", "nodes", "leaves", "gemm_flops", "fwd_spectra",
-                 "inv_spectra", "surface_interactions")
+                 "inv_spectra", "surface_interactions", "tc_hadamard_flops")
         return {names[i]: c[i] for i in range(n.value)}
 
     def last_launch_count(self) -> int:
