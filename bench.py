@@ -7,8 +7,9 @@ seeded synthetic data (no dataset is involved).  A step is one FMM3d::eval
 (device-resident densities in, device-resident potentials out) of that whole
 point cloud; setup (tree, lists, operators) is done once, outside timing.
 
-  value      Mpoints/s of the mixed-precision engine (FP32 bulk, surface
-             contractions in split TF32 on the tensor cores), all ranks together
+  value      Mpoints/s of the mixed-precision engine (FP32 point sums and
+             spectra, V-list Hadamard and surface contractions in split TF32
+             on the tensor cores), all ranks together
   fp64       the plain FP64 GPU engine on the same workload
   batched    64 independent instances (48 Laplace + 16 Stokes single-layer,
              np=6, log-uniform sizes in [1e4, 5e5], sphere / cube / Plummer
@@ -22,6 +23,11 @@ point cloud; setup (tree, lists, operators) is done once, outside timing.
   cpu_baseline  the reference's own CPU eval (oracle/_ref, built from the
              reference sources) on a 65,536-point sample of the same cloud,
              one host thread, rank 0 at N=1 only
+  roofline   the dominant kernel, k_m2l_had_tc (V-list Hadamard): algorithmic
+             flops (8 per V-list pair and stored frequency) over its CUDA-event
+             time against the TF32 dense rate (half the measured bf16 rate),
+             with the executed tensor rate, the algorithmic HBM rate and the
+             DRAM traffic scaled from an ncu capture beside it
 
 --impl reference runs the reference's CPU eval instead, one process per host
 core on independent 65,536-point samples, and reports their aggregate.
