@@ -1,7 +1,7 @@
 /* Test infrastructure (oracle only) -- never linked into the product.
  *
  * A plain-C CPU restatement of the reference KIFMM pieces that parity is
- * judged on:
+ * checked against:
  *   - the kernel library and the FP64 direct sum
  *       Kernel3d::kernel   fmm3d/kernel3d.cpp:116-414
  *       Dense3d::eval      fmm3d/dense3d.cpp:38-57
