@@ -302,6 +302,55 @@ class Batch:
             self._b = None
 
 
+def fmm3d_mex(srcpos, srcnor, trgpos, ctr, rootlvl, knl, np_, srcden, numchk: int = 20, precision: str = "fp64",
+              return_check: bool = False):
+    """The reference's MATLAB entry point (fmm3d/fmm3d_mex.cpp:13-64) with its
+    8 arguments, over the same engine:
+
+        trgval = fmm3d_mex(srcpos, srcnor, trgpos, ctr, rootlvl, knl, np, srcden)
+
+    srcpos, srcnor: 3 x ns, trgpos: 3 x nt (MATLAB's column-major DblNumMat);
+    ctr: 3 values; rootlvl: int; knl: (kt, coefs) like the 2 x 1 cell
+    {kt; coefs} (or a Kernel3d); np in {4, 6, 8}; srcden: sdof * ns values.
+    Options as the MEX file sets them: ptsmax 150, maxlevel 10 (:32-46).
+    Returns trgval (tdof * nt values); the check against the direct sum at
+    numchk targets (:59) is returned beside it when return_check is true.
+
+    Differences from the MEX file, whose own code does not do what its
+    arguments say: it passes srcpos as the normals and ignores ctr and rootlvl
+    (:51-52); here srcnor, ctr and rootlvl are used.  Its iA asserts (np, the
+    density size) raise ValueError."""
+    if int(np_) not in (4, 6, 8):
+        raise ValueError("np must be 4, 6 or 8")
+    k = knl if isinstance(knl, Kernel3d) else Kernel3d(int(knl[0]), knl[1])
+
+    def cols(a, name):
+        a = np.asarray(a, dtype=np.float64)
+        if a.ndim != 2 or a.shape[0] != 3:
+            raise ValueError(f"{name} must be 3 x n")
+        return np.ascontiguousarray(a.T)
+
+    sp, sn, tp = cols(srcpos, "srcpos"), cols(srcnor, "srcnor"), cols(trgpos, "trgpos")
+    if sn.shape != sp.shape:
+        raise ValueError("srcnor must have the shape of srcpos")
+    den = np.ascontiguousarray(srcden, dtype=np.float64).ravel()
+    if den.size != k.sdof() * len(sp):
+        raise ValueError("srcden must have sdof * ns values")
+    c = np.asarray(ctr, dtype=np.float64).ravel()
+    if c.size != 3:
+        raise ValueError("ctr must have 3 values")
+    fmm = FMM3d("fmm3d_")
+    fmm.srcpos, fmm.srcnor, fmm.trgpos = sp, sn, tp
+    fmm.ctr, fmm.rootlvl = (float(c[0]), float(c[1]), float(c[2])), int(rootlvl)
+    fmm.knl = k
+    fmm.setup({"-fmm3d_np": str(int(np_)), "-fmm3d_let3d_ptsmax": "150", "-fmm3d_let3d_maxlevel": "10",
+               "-fmm3d_precision": precision})
+    trgval = np.zeros(k.tdof() * len(tp))
+    fmm.eval(den, trgval)
+    rel = fmm.check(den, trgval, numchk) if numchk > 0 else None
+    return (trgval, rel) if return_check else trgval
+
+
 def header_symbols(header_path: str | None = None):
     """Entry points declared in include/kifmm.h (for the ABI test)."""
     import re

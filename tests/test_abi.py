@@ -154,3 +154,25 @@ def test_empty_target_and_source_sets():
     f = make(n=0)
     assert setup_ok(f) in (True, False)
     assert f.tree()["depth"].tolist() == [0]
+
+
+def test_mex_front_end_checks_its_arguments():
+    """fmm3d_mex mirrors fmm3d/fmm3d_mex.cpp's 8 arguments; its asserts
+    (np in {4, 6, 8}, srcden size, 3 x n matrices) raise before any device
+    work, and valid arguments reach setup (KIFMM_ERR_NO_DEVICE without a GPU)."""
+    rng = np.random.default_rng(3)
+    p = rng.uniform(-1, 1, (3, 200))
+    den = rng.uniform(-1, 1, 200)
+    with pytest.raises(ValueError):
+        kifmm.fmm3d_mex(p, p, p, (0, 0, 0), 0, (111, [1.0]), 5, den)
+    with pytest.raises(ValueError):
+        kifmm.fmm3d_mex(p, p, p, (0, 0, 0), 0, (111, [1.0]), 4, den[:-1])
+    with pytest.raises(ValueError):
+        kifmm.fmm3d_mex(p.T, p.T, p.T, (0, 0, 0), 0, (111, [1.0]), 4, den)
+    with pytest.raises(ValueError):
+        kifmm.fmm3d_mex(p, p, p, (0, 0), 0, (111, [1.0]), 4, den)
+    try:
+        out = kifmm.fmm3d_mex(p, p, p, (0, 0, 0), 0, (111, [1.0]), 4, den)
+        assert out.shape == (200,)
+    except kifmm.KifmmError as e:
+        assert e.status == kifmm.KIFMM_ERR_NO_DEVICE, e

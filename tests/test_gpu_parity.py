@@ -271,3 +271,21 @@ def test_tensor_core_hadamard_matches_toeplitz_form(gpu, name):
         assert diff == 0.0, diff
     else:
         assert diff <= 5e-6, diff
+
+
+def test_mex_front_end_matches_the_object_api(gpu):
+    """fmm3d_mex (the reference's 8-argument MATLAB entry point) gives the
+    FMM3d object's result bit for bit, with the MEX file's options (ptsmax
+    150, maxlevel 10), and its check error stays at the FMM error."""
+    d = G.load("lap_s_np6_tt_style")
+    f = kifmm.FMM3d("fmm3d_")
+    f.srcpos, f.srcnor, f.trgpos = d["src"], d["nor"], d["trg"]
+    f.ctr, f.rootlvl = tuple(d["ctr"]), d["rootlvl"]
+    f.knl = kifmm.Kernel3d(d["kt"], d["coefs"])
+    f.setup({"-fmm3d_np": "6", "-fmm3d_let3d_ptsmax": "150", "-fmm3d_let3d_maxlevel": "10"})
+    ref = np.zeros(len(d["trg"]))
+    f.eval(d["den"], ref)
+    out, rel = kifmm.fmm3d_mex(d["src"].T, d["nor"].T, d["trg"].T, d["ctr"], d["rootlvl"], (d["kt"], d["coefs"]), 6,
+                               d["den"], return_check=True)
+    assert np.array_equal(out, ref)
+    assert rel < 1e-4, rel
