@@ -180,6 +180,73 @@ struct WarpSrc64 {  // one staged batch of 64 sources
   T n[64 * 3];
 };
 
+// Single-dof Laplace sums in FP32 run on packed f32x2 arithmetic, two
+// sources per instruction: the staged batch is then pair-interleaved,
+// pair q = sources 2q, 2q + 1 as {x0, x1, y0, y1} {z0, z1, w0, w1}, so one
+// pair is two 16-byte shared loads already in packed-register order.
+template <typename T>
+__device__ __forceinline__ void stage_src(WarpSrc64<T>& w, int j, P4<T> v, bool paired) {
+  if (!paired) {
+    w.p[j] = v;
+    return;
+  }
+  T* q = reinterpret_cast<T*>(w.p) + 8 * (j >> 1) + (j & 1);
+  q[0] = v.x;
+  q[2] = v.y;
+  q[4] = v.z;
+  q[6] = v.w;
+}
+
+__device__ __forceinline__ unsigned long long pk2(float lo, float hi) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void upk2(unsigned long long v, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ unsigned long long sub2(unsigned long long a, unsigned long long b) {
+  unsigned long long r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ unsigned long long mul2(unsigned long long a, unsigned long long b) {
+  unsigned long long r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ unsigned long long fma2(unsigned long long a, unsigned long long b, unsigned long long c) {
+  unsigned long long r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
+
+// sum over the pairs q = sg, sg + nsplit, ... < npairs of w / |t - s| (the
+// 1e-16 cut-off as in keval), for target t = (px, py, pz)
+__device__ __forceinline__ float lap_pairs(const WarpSrc64<float>& w, float px, float py, float pz, int sg,
+                                           int nsplit, int npairs) {
+  const float4* wp = reinterpret_cast<const float4*>(w.p);
+  const unsigned long long PX = pk2(px, px), PY = pk2(py, py), PZ = pk2(pz, pz);
+  unsigned long long S = pk2(0.f, 0.f);
+  const int rounds = sg < npairs ? (npairs - sg + nsplit - 1) / nsplit : 0;
+#pragma unroll 4
+  for (int r = 0; r < rounds; r++) {
+    const int q = sg + r * nsplit;
+    const float4 A = wp[2 * q], B = wp[2 * q + 1];
+    const unsigned long long X = sub2(PX, pk2(A.x, A.y)), Y = sub2(PY, pk2(A.z, A.w)), Z = sub2(PZ, pk2(B.x, B.y));
+    unsigned long long R2 = mul2(X, X);
+    R2 = fma2(Y, Y, R2);
+    R2 = fma2(Z, Z, R2);
+    float r2a, r2b;
+    upk2(R2, r2a, r2b);
+    const float ria = (r2a >= 1e-16f) ? rsqrt_t(r2a) : 0.f, rib = (r2b >= 1e-16f) ? rsqrt_t(r2b) : 0.f;
+    S = fma2(pk2(ria, rib), pk2(B.z, B.w), S);
+  }
+  float sa, sb;
+  upk2(S, sa, sb);
+  return sa + sb;
+}
+
 // S2M: lane l owns upward check points l, l + 32, ... (R rounds); every
 // staged source (a broadcast load) updates all of them.
 template <typename T, int KT, int R>
@@ -287,6 +354,8 @@ __global__ void __launch_bounds__(32 * NWARP) k_leaf_warp(P2PArgs<T> a, const in
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   WarpSrc64<T>& w = ws[warp];
   WarpSegs<T>& sgt = wg[warp];
+  // packed FP32 Laplace sums (near field for KT 111, surfaces for MM 111)
+  constexpr bool PAIR_NEAR = KT == 111 && sizeof(T) == 4, PAIR_SURF = MM == 111 && sizeof(T) == 4;
   const T* den = a.sden + (size_t)rhs * a.ns * SD;
   T* outbase = a.tval + (size_t)rhs * a.nt * TD;
   const int nsurf = a.nsurf;
@@ -341,7 +410,11 @@ __global__ void __launch_bounds__(32 * NWARP) k_leaf_warp(P2PArgs<T> a, const in
 #pragma unroll
           for (int h = 0; h < 2; h++) {
             const int jl = lane + 32 * h;
-            if (jl >= cnt) break;
+            if (jl >= cnt) {
+              // an odd batch's last pair: a zero-weight partner
+              if (PAIR_NEAR && jl == cnt && (cnt & 1)) stage_src(w, jl, P4<T>{T(0), T(0), T(0), T(0)}, true);
+              break;
+            }
             const int k = k0 + jl;
             int lo = 0, hi = nseg;  // pre[lo] <= k < pre[hi]
             while (hi - lo > 1) {
@@ -355,7 +428,8 @@ __global__ void __launch_bounds__(32 * NWARP) k_leaf_warp(P2PArgs<T> a, const in
             T f[SD];
 #pragma unroll
             for (int s = 0; s < SD; s++) f[s] = den[(size_t)p * SD + s];
-            w.p[jl] = P4<T>{a.sx[p] + sgt.shx[lo], a.sy[p] + sgt.shy[lo], a.sz[p] + sgt.shz[lo], f[0]};
+            stage_src(w, jl, P4<T>{a.sx[p] + sgt.shx[lo], a.sy[p] + sgt.shy[lo], a.sz[p] + sgt.shz[lo], f[0]},
+                      PAIR_NEAR);
 #pragma unroll
             for (int s = 1; s < SD; s++) w.f[jl * (SD - 1) + s - 1] = f[s];
             if constexpr (DL) {
@@ -367,7 +441,9 @@ __global__ void __launch_bounds__(32 * NWARP) k_leaf_warp(P2PArgs<T> a, const in
           __syncwarp();
           if (valid) {
             const int rounds = sg < cnt ? (cnt - sg + nsplit - 1) / nsplit : 0;
-            if constexpr (KT == 111) {  // sum f / r, times 1/(4 pi) once
+            if constexpr (PAIR_NEAR) {  // sum f / r on source pairs, times 1/(4 pi) once
+              acc[0] += a.ku.c0 * lap_pairs(w, px, py, pz, sg, nsplit, (cnt + 1) >> 1);
+            } else if constexpr (KT == 111) {  // FP64: sum f / r, times 1/(4 pi) once
               T s1 = T(0);
 #pragma unroll 4
               for (int r = 0; r < rounds; r++) {
@@ -429,21 +505,28 @@ __global__ void __launch_bounds__(32 * NWARP) k_leaf_warp(P2PArgs<T> a, const in
 #pragma unroll
           for (int h = 0; h < 2; h++) {
             const int jl = lane + 32 * h;
-            if (jl >= cnt) break;
+            if (jl >= cnt) {
+              if (PAIR_SURF && jl == cnt && (cnt & 1)) stage_src(w, jl, P4<T>{T(0), T(0), T(0), T(0)}, true);
+              break;
+            }
             const int k = k0 + jl;
             const int e = k / nsurf, m = k - e * nsurf;
             const T* u = sgt.unit[e];
             const T* sd = sgt.den[e];
             const T r = sgt.rad[e];
-            w.p[jl] = P4<T>{u[3 * m] * r + sgt.shx[e], u[3 * m + 1] * r + sgt.shy[e], u[3 * m + 2] * r + sgt.shz[e],
-                             sd[(size_t)m * SDM]};
+            stage_src(w, jl,
+                      P4<T>{u[3 * m] * r + sgt.shx[e], u[3 * m + 1] * r + sgt.shy[e], u[3 * m + 2] * r + sgt.shz[e],
+                            sd[(size_t)m * SDM]},
+                      PAIR_SURF);
 #pragma unroll
             for (int s = 1; s < SDM; s++) w.f[jl * (SDM - 1) + s - 1] = sd[(size_t)m * SDM + s];
           }
           __syncwarp();
           if (valid) {
             const int rounds = sg < cnt ? (cnt - sg + nsplit - 1) / nsplit : 0;
-            if constexpr (MM == 111) {
+            if constexpr (PAIR_SURF) {
+              acc[0] += a.km.c0 * lap_pairs(w, px, py, pz, sg, nsplit, (cnt + 1) >> 1);
+            } else if constexpr (MM == 111) {
               T s1 = T(0);
 #pragma unroll 4
               for (int r = 0; r < rounds; r++) {
