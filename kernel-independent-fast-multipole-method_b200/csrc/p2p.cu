@@ -275,6 +275,20 @@ __global__ void __launch_bounds__(32 * WP_WARPS) k_s2m_warp(P2PArgs<T> a, const 
 #pragma unroll
       for (int d = 0; d < TD; d++) acc[r][d] = T(0);
     }
+    // FP32 Laplace: packed f32x2 sums over pairs of this lane's check points
+    constexpr bool PACKED = KT == 111 && sizeof(T) == 4;
+    unsigned long long PX[R / 2 > 0 ? R / 2 : 1], PY[R / 2 > 0 ? R / 2 : 1], PZ[R / 2 > 0 ? R / 2 : 1],
+        SP[R / 2 > 0 ? R / 2 : 1];
+    float s_last = 0.f;
+    if constexpr (PACKED) {
+#pragma unroll
+      for (int rp = 0; rp < R / 2; rp++) {
+        PX[rp] = pk2(px[2 * rp], px[2 * rp + 1]);
+        PY[rp] = pk2(py[2 * rp], py[2 * rp + 1]);
+        PZ[rp] = pk2(pz[2 * rp], pz[2 * rp + 1]);
+        SP[rp] = pk2(0.f, 0.f);
+      }
+    }
     for (int c0 = 0; c0 < sc; c0 += 32) {
       const int cnt = min(32, sc - c0);
       __syncwarp();
@@ -310,10 +324,45 @@ __global__ void __launch_bounds__(32 * WP_WARPS) k_s2m_warp(P2PArgs<T> a, const 
           nrm[1] = w.n[3 * j + 1];
           nrm[2] = w.n[3 * j + 2];
         }
+        if constexpr (PACKED) {
+          // check points 2 rp, 2 rp + 1 as one f32x2 pair; an odd last round scalar
+          const unsigned long long SX = pk2(sp.x, sp.x), SY = pk2(sp.y, sp.y), SZ = pk2(sp.z, sp.z),
+                                   SW = pk2(sp.w, sp.w);
 #pragma unroll
-        for (int r = 0; r < R; r++)
-          if (32 * r < nt) keval<KT, T>(px[r] - sp.x, py[r] - sp.y, pz[r] - sp.z, nrm, f, acc[r], a.ku);
+          for (int rp = 0; rp < R / 2; rp++) {
+            if (64 * rp >= nt) break;
+            const unsigned long long X = sub2(PX[rp], SX), Y = sub2(PY[rp], SY), Z = sub2(PZ[rp], SZ);
+            unsigned long long R2 = mul2(X, X);
+            R2 = fma2(Y, Y, R2);
+            R2 = fma2(Z, Z, R2);
+            float r2a, r2b;
+            upk2(R2, r2a, r2b);
+            const float ria = (r2a >= 1e-16f) ? rsqrt_t(r2a) : 0.f, rib = (r2b >= 1e-16f) ? rsqrt_t(r2b) : 0.f;
+            SP[rp] = fma2(pk2(ria, rib), SW, SP[rp]);
+          }
+          if constexpr (R % 2 == 1) {
+            if (32 * (R - 1) < nt) {
+              const float x = px[R - 1] - sp.x, y = py[R - 1] - sp.y, z = pz[R - 1] - sp.z;
+              const float r2 = x * x + y * y + z * z;
+              s_last += ((r2 >= 1e-16f) ? rsqrt_t(r2) : 0.f) * sp.w;
+            }
+          }
+        } else {
+#pragma unroll
+          for (int r = 0; r < R; r++)
+            if (32 * r < nt) keval<KT, T>(px[r] - sp.x, py[r] - sp.y, pz[r] - sp.z, nrm, f, acc[r], a.ku);
+        }
       }
+    }
+    if constexpr (PACKED) {  // sum f / r, times 1/(4 pi) once
+#pragma unroll
+      for (int rp = 0; rp < R / 2; rp++) {
+        float sa, sb;
+        upk2(SP[rp], sa, sb);
+        acc[2 * rp][0] = a.ku.c0 * sa;
+        acc[2 * rp + 1][0] = a.ku.c0 * sb;
+      }
+      if constexpr (R % 2 == 1) acc[R - 1][0] = a.ku.c0 * s_last;
     }
     T* outbase = a.supcval + (size_t)g * nt * TD;
 #pragma unroll
