@@ -229,7 +229,7 @@ __device__ __forceinline__ float lap_pairs(const WarpSrc64<float>& w, float px, 
   const unsigned long long PX = pk2(px, px), PY = pk2(py, py), PZ = pk2(pz, pz);
   unsigned long long S = pk2(0.f, 0.f);
   const int rounds = sg < npairs ? (npairs - sg + nsplit - 1) / nsplit : 0;
-#pragma unroll 4
+#pragma unroll 8
   for (int r = 0; r < rounds; r++) {
     const int q = sg + r * nsplit;
     const float4 A = wp[2 * q], B = wp[2 * q + 1];
