@@ -58,6 +58,13 @@ __host__ __device__ inline size_t fwd_warp_bytes(int np, int n, int nh) {
          align16(sizeof(Cpx<T>) * np * n * nh);
 }
 
+// register-blocked forward: A (np x np x nh) and Bm (np x n x nh) per warp; the
+// density grid (np^3) shares Bm's space, being dead before the y pass writes Bm
+template <typename T>
+__host__ __device__ inline size_t fwd_rb_warp_bytes(int np, int n, int nh) {
+  return align16(sizeof(Cpx<T>) * np * np * nh) + align16(sizeof(Cpx<T>) * np * n * nh);
+}
+
 // register-blocked inverse: Bm (np x n x nh) and A (np x np x nh) per warp
 template <typename T>
 __host__ __device__ inline size_t inv_rb_warp_bytes(int np, int n, int nh) {
@@ -373,10 +380,13 @@ __global__ void __launch_bounds__(256) k_m2l_fwd_rb(M2LGeom g, const T* __restri
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpc = blockDim.x >> 5;
   int* c_of = reinterpret_cast<int*>(smem_raw);  // full -> compact frequency index (< 0: not stored)
   for (int e = threadIdx.x; e < N * N * NH; e += blockDim.x) c_of[e] = g.ff2c[e];
-  unsigned char* mine = smem_raw + align16(sizeof(int) * N * N * NH) + (size_t)warp * fwd_warp_bytes<T>(NP, N, NH);
-  T* xg = reinterpret_cast<T*>(mine);
-  Cpx<T>* A = reinterpret_cast<Cpx<T>*>(mine + align16(sizeof(T) * NP * NP * NP));
-  Cpx<T>* Bm = reinterpret_cast<Cpx<T>*>(reinterpret_cast<unsigned char*>(A) + align16(sizeof(Cpx<T>) * NP * NP * NH));
+  unsigned char* mine = smem_raw + align16(sizeof(int) * N * N * NH) + (size_t)warp * fwd_rb_warp_bytes<T>(NP, N, NH);
+  Cpx<T>* A = reinterpret_cast<Cpx<T>*>(mine);
+  Cpx<T>* Bm = reinterpret_cast<Cpx<T>*>(mine + align16(sizeof(Cpx<T>) * NP * NP * NH));
+  // the density grid lives in Bm's space: read only by the x pass, which a
+  // __syncwarp separates from the y pass's first write of Bm
+  T* xg = reinterpret_cast<T*>(Bm);
+  static_assert(sizeof(T) * NP * NP * NP <= sizeof(Cpx<T>) * NP * N * NH, "density grid fits in Bm");
   __syncthreads();
   for (int wi = blockIdx.x * wpc + warp; wi < nwork; wi += gridDim.x * wpc) {
     const int node = nodes[wi];
@@ -563,8 +573,9 @@ void launch_m2l_forward(const M2LGeom& g, const T* supeden, const int* nodes, in
   int grid = std::max(1, std::min((nn + wpc - 1) / wpc, 148 * 8));
   if (g.np == 4 || g.np == 6 || g.np == 8) {
     const size_t head_rb = align16(sizeof(int) * g.n * g.n * g.nh);
-    const int w = (int)std::max<size_t>(1, std::min<size_t>(8, (200 * 1024 - head_rb) / per_warp));
-    const size_t sm = head_rb + per_warp * w;
+    const size_t per_rb = fwd_rb_warp_bytes<T>(g.np, g.n, g.nh);
+    const int w = (int)std::max<size_t>(1, std::min<size_t>(8, (200 * 1024 - head_rb) / per_rb));
+    const size_t sm = head_rb + per_rb * w;
     const int gr = std::max(1, std::min((nn + w - 1) / w, 148 * 8));
     auto kern = g.np == 6 ? k_m2l_fwd_rb<T, 6> : g.np == 4 ? k_m2l_fwd_rb<T, 4> : k_m2l_fwd_rb<T, 8>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
