@@ -43,7 +43,10 @@
 //               order (a group that skipped a phase of a shared stage could
 //               match the parity of a phase two behind); the group also
 //               issues the step's operator copy (operator stage s mod 6) and
-//               arrives on afull only once it has landed
+//               arrives on afull only once it has landed.  A group walks its
+//               own steps only (s to s + 3 directly): every instruction it
+//               spends between two of its steps lengthens the round trip of
+//               its A stage, which with three stages sets the step rate
 //   warps 12-15 MMA warps: warp 12 + f issues frequency f's 4 MMAs of every
 //               step (its own accumulator columns; one elected lane) and
 //               commits; at an item's end it drains TMEM lane quarter
@@ -334,68 +337,72 @@ __global__ void __launch_bounds__(HT_THREADS, 1)
         nb[k] = q < nq ? __ldg(coll + (size_t)q * 26 + x.d) : zero_node;
       }
     };
+    // the group walks its own steps only, s = grp, grp + 3, ...: from step s
+    // it goes to s + 3 directly, and fetches the colleague indices of s + 3
+    // as soon as step s's spectra loads are issued, a whole round of the
+    // three groups before they are used
     StepIter it;
     start(it, 0);
-    int s = 0, pend = -1;  // pend: step of an operator copy not yet seen landed
-    int nb[4];             // colleague indices of this group's next step, fetched a step early
-    bool have_nb = false;
-    while (next(it)) {
-      const int stg = s % HT_ASTAGES;
-      if (stg != grp) {
-        if ((s + 1) % HT_ASTAGES == grp) {  // the next step is this group's
-          StepIter nx = it;
-          have_nb = next(nx);
-          if (have_nb) load_nb(nx, nb);
-        }
-      } else {
-        if (!have_nb) load_nb(it, nb);
-        have_nb = false;
-        // the step's operator images into stage s mod 6, last read by step
-        // s - 6, whose MMAs completed before this group's stage wait of step
-        // s - 3 (stages s mod 6 and s + 3 mod 6 belong to this group alone)
-        if (qd == 0 && lane == 0) {
-          bulk_load(smem_u32(smem + (size_t)(s % HT_NB) * HT_IMG_BYTES),
-                    img + ((size_t)it.fc * 26 + it.d) * HT_IMG_FLOATS, HT_IMG_BYTES, smem_u32(&bfull[s % HT_NB]));
-        }
-        if (qd == 0) pend = s;
-        // v[h][ab][kh]: 4 complex (frequencies f0 .. f0 + 3) of child 4 kh + c
-        // of the colleague of row 32 qd + 16 h + 8 ab + t / 4
-        float v[2][2][2][8];
-#pragma unroll
-        for (int h = 0; h < 2; h++)
-#pragma unroll
-          for (int ab = 0; ab < 2; ab++) {
-            // the colleague's block of this chunk: 8 children x 4 frequencies
-            const float* row = spectra + (((size_t)((nb[2 * h + ab] + 7) >> 3) * (NF / HT_F) + it.fc) * 8 + c) * 8;
-            ld32B(row, v[h][ab][0]);
-            ld32B(row + 32, v[h][ab][1]);
-          }
-        if (s >= HT_ASTAGES && !wait(&aempty[stg], ((s / HT_ASTAGES) + 1) & 1)) break;
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const unsigned abase = tmem + HT_ACOL0 + (unsigned)stg * (HT_F * 32);
-        // frequency f: column blocks f*32 + {head kh 0, head kh 1, tail kh 0,
-        // tail kh 1}; block column 2 (t % 4) + (re, im) = child 4 kh + t % 4
-#pragma unroll
-        for (int h = 0; h < 2; h++)
-#pragma unroll
-          for (int f = 0; f < HT_F; f++) {
-            unsigned r[16];
-#pragma unroll
-            for (int kh = 0; kh < 2; kh++)
-#pragma unroll
-              for (int ab = 0; ab < 2; ab++)
-                split_hl2(v[h][ab][kh][2 * f], v[h][ab][kh][2 * f + 1], &r[4 * kh + 2 * ab], &r[8 + 4 * kh + 2 * ab]);
-            tmem_st16x256_x4(abase + ((unsigned)(qd * 32 + 16 * h) << 16) + f * 32, r);
-          }
-        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        if (qd == 0) {
-          if (!wait(&bfull[s % HT_NB], (s / HT_NB) & 1)) break;
-          pend = -1;
-        }
-        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&afull[stg])) : "memory");
+    bool ok = true;
+    for (int k = 0; k <= grp && ok; k++) ok = next(it);
+    int s = grp, pend = -1;  // pend: step of an operator copy not yet seen landed
+    int nb[4];               // colleague first children of this thread's rows at step s
+    if (ok) load_nb(it, nb);
+    while (ok) {
+      // the step's operator images into stage s mod 6, last read by step
+      // s - 6, whose MMAs completed before this group's stage wait of step
+      // s - 3 (stages s mod 6 and s + 3 mod 6 belong to this group alone)
+      if (qd == 0 && lane == 0) {
+        bulk_load(smem_u32(smem + (size_t)(s % HT_NB) * HT_IMG_BYTES),
+                  img + ((size_t)it.fc * 26 + it.d) * HT_IMG_FLOATS, HT_IMG_BYTES, smem_u32(&bfull[s % HT_NB]));
       }
-      s++;
+      if (qd == 0) pend = s;
+      // v[h][ab][kh]: 4 complex (frequencies f0 .. f0 + 3) of child 4 kh + c
+      // of the colleague of row 32 qd + 16 h + 8 ab + t / 4
+      float v[2][2][2][8];
+#pragma unroll
+      for (int h = 0; h < 2; h++)
+#pragma unroll
+        for (int ab = 0; ab < 2; ab++) {
+          // the colleague's block of this chunk: 8 children x 4 frequencies
+          const float* row = spectra + (((size_t)((nb[2 * h + ab] + 7) >> 3) * (NF / HT_F) + it.fc) * 8 + c) * 8;
+          ld32B(row, v[h][ab][0]);
+          ld32B(row + 32, v[h][ab][1]);
+        }
+      // the group's next step and its colleague indices (nb is free once the
+      // loads above are issued)
+      StepIter nx = it;
+      bool okn = next(nx);
+      if (okn) okn = next(nx);
+      if (okn) okn = next(nx);
+      if (okn) load_nb(nx, nb);
+      if (s >= HT_ASTAGES && !wait(&aempty[grp], ((s / HT_ASTAGES) + 1) & 1)) break;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const unsigned abase = tmem + HT_ACOL0 + (unsigned)grp * (HT_F * 32);
+      // frequency f: column blocks f*32 + {head kh 0, head kh 1, tail kh 0,
+      // tail kh 1}; block column 2 (t % 4) + (re, im) = child 4 kh + t % 4
+#pragma unroll
+      for (int h = 0; h < 2; h++)
+#pragma unroll
+        for (int f = 0; f < HT_F; f++) {
+          unsigned r[16];
+#pragma unroll
+          for (int kh = 0; kh < 2; kh++)
+#pragma unroll
+            for (int ab = 0; ab < 2; ab++)
+              split_hl2(v[h][ab][kh][2 * f], v[h][ab][kh][2 * f + 1], &r[4 * kh + 2 * ab], &r[8 + 4 * kh + 2 * ab]);
+          tmem_st16x256_x4(abase + ((unsigned)(qd * 32 + 16 * h) << 16) + f * 32, r);
+        }
+      asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      if (qd == 0) {
+        if (!wait(&bfull[s % HT_NB], (s / HT_NB) & 1)) break;
+        pend = -1;
+      }
+      asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&afull[grp])) : "memory");
+      it = nx;
+      ok = okn;
+      s += HT_ASTAGES;
     }
     // after a time-out: the copy this warp issued last has landed before the CTA ends
     if (pend >= 0) mbar_wait_bounded(smem_u32(&bfull[pend % HT_NB]), (pend / HT_NB) & 1);
