@@ -282,6 +282,24 @@ __global__ void __launch_bounds__(HT_THREADS, 1)
     return false;
   };
   auto last_of_item = [&](const StepIter& it) { return it.d >= 25 || (it.dm >> (it.d + 1)) == 0u; };
+  // advance three steps: inside an item, the third set bit of the direction
+  // mask above d (two bit clears and one find-first-set); across an item's
+  // end, three single steps
+  auto next3 = [&](StepIter& it) {
+    if (it.d < 25) {
+      unsigned r = it.dm >> (it.d + 1);
+      r &= r - 1u;
+      r &= r - 1u;
+      if (r) {
+        it.d += __ffs(r);
+        return true;
+      }
+    }
+    bool o = next(it);
+    if (o) o = next(it);
+    if (o) o = next(it);
+    return o;
+  };
 
   // drain item li from TMEM lane quarter (warp & 3) into effval: wait for the
   // item's MMAs, read the four frequencies' accumulators, release them,
@@ -372,9 +390,7 @@ __global__ void __launch_bounds__(HT_THREADS, 1)
       // the group's next step and its colleague indices (nb is free once the
       // loads above are issued)
       StepIter nx = it;
-      bool okn = next(nx);
-      if (okn) okn = next(nx);
-      if (okn) okn = next(nx);
+      const bool okn = next3(nx);
       if (okn) load_nb(nx, nb);
       if (s >= HT_ASTAGES && !wait(&aempty[grp], ((s / HT_ASTAGES) + 1) & 1)) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
