@@ -468,8 +468,10 @@ def engine_arm(args):
                      "algorithmic": "8 flops per V-list pair and stored frequency",
                      "executed_tensor_tflops": had_exec_flops / (had_ms / 1e3) / 1e12,
                      "hbm_achieved_gbs": alg_bytes / (had_ms / 1e3) / 1e9, "hbm_peak_gbs": hbm,
-                     "limiter": "latency of the colleague-spectra gather into the producer warps (long_scoreboard "
-                                "stalls; tensor pipe ~18 % active, DRAM ~8 % of peak in the ncu capture)"},
+                     "limiter": "round trip of each producer group's TMEM A stage (gather loads, wait for the "
+                                "stage's previous MMAs, split and store, operator images), one third of it per "
+                                "step with three stages; neither the tensor pipe (~18 % active) nor DRAM (~8 % "
+                                "of peak) is saturated"},
         "clocks": clk,
         "cpu_baseline": cpu,
     }
