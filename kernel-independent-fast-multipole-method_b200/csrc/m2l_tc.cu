@@ -281,7 +281,6 @@ __global__ void __launch_bounds__(HT_THREADS, 1)
     }
     return false;
   };
-  auto last_of_item = [&](const StepIter& it) { return it.d >= 25 || (it.dm >> (it.d + 1)) == 0u; };
   // advance three steps: inside an item, the third set bit of the direction
   // mask above d (two bit clears and one find-first-set); across an item's
   // end, three single steps
@@ -425,29 +424,43 @@ __global__ void __launch_bounds__(HT_THREADS, 1)
   } else {
     // ---- MMA warps: warp HT_MMA_WARP + f, frequency f.  The next step's
     // afull is tested (without blocking) before this step's MMAs go out, so
-    // the test's latency hides behind them
+    // the test's latency hides behind them.  The warps go item by item: an
+    // item's step count is the population count of its tile's direction mask
+    // (loaded one item ahead), so a step costs no walk of the mask
     const int f = warp - HT_MMA_WARP;
-    StepIter it;
-    start(it, 0);
+    auto tile_of = [&](int li) {
+      const int i = blockIdx.x + li * gridDim.x;
+      return i - (i / ntiles) * ntiles;
+    };
     int s = 0;
-    bool first = true;   // first step of an item
     bool ready = false;  // afull of step s seen complete
-    while (next(it)) {
-      const int stg = s % HT_ASTAGES;
-      if (!__all_sync(0xffffffffu, ready) && !wait(&afull[stg], (s / HT_ASTAGES) & 1)) break;
-      if (first && it.li >= 1 && !wait(&accempty, (it.li - 1) & 1)) break;
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const int s1 = s + 1;
-      ready = mbar_test(smem_u32(&afull[s1 % HT_ASTAGES]), (s1 / HT_ASTAGES) & 1);
-      mma_freq(tmem + f * 32, tmem + HT_ACOL0 + (unsigned)stg * (HT_F * 32) + f * 32,
-               img_desc(smem_u32(smem + (size_t)(s % HT_NB) * HT_IMG_BYTES + f * 2048)), first ? 0 : 1);
-      commit_elect(smem_u32(&aempty[stg]));
-      first = last_of_item(it);
-      s++;
-      if (first) {
-        commit_elect(smem_u32(&accfull));
-        if (!drain(it.li)) break;  // lane quarter warp mod 4 of the item just finished
+    bool failed = false;
+    unsigned dm_next = __ldg(tile_dirs + tile_of(0));
+    for (int li = 0; li < my_items; li++) {
+      const unsigned dm = dm_next;
+      if (li + 1 < my_items) dm_next = __ldg(tile_dirs + tile_of(li + 1));
+      const int nst = __popc(dm);
+      for (int k = 0; k < nst; k++) {
+        const int stg = s % HT_ASTAGES;
+        if (!__all_sync(0xffffffffu, ready) && !wait(&afull[stg], (s / HT_ASTAGES) & 1)) {
+          failed = true;
+          break;
+        }
+        if (k == 0 && li >= 1 && !wait(&accempty, (li - 1) & 1)) {
+          failed = true;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const int s1 = s + 1;
+        ready = mbar_test(smem_u32(&afull[s1 % HT_ASTAGES]), (s1 / HT_ASTAGES) & 1);
+        mma_freq(tmem + f * 32, tmem + HT_ACOL0 + (unsigned)stg * (HT_F * 32) + f * 32,
+                 img_desc(smem_u32(smem + (size_t)(s % HT_NB) * HT_IMG_BYTES + f * 2048)), k == 0 ? 0 : 1);
+        commit_elect(smem_u32(&aempty[stg]));
+        s++;
       }
+      if (failed) break;
+      commit_elect(smem_u32(&accfull));
+      if (!drain(li)) break;  // lane quarter warp mod 4 of the item just finished
     }
     // before the CTA ends every MMA issued has completed (only a time-out
     // leaves any outstanding)
