@@ -84,6 +84,18 @@ struct Impl : ImplBase {
 
   int sd_u, td_u, sd_m, td_m, nsurf, nuc;
   P2PArgs<T> args;
+  // Double-layer kernels in mixed precision: the U-list sums in FP64.  For
+  // two sources closer than their leaf's size the double-layer factor r.n is
+  // O(|r|^2) and comes out of the FP32 coordinates with an error of the
+  // leaf size times 2^-24, which near-coincident pairs turn into a relative
+  // error of order one in their term (0.27 at 262,144 points on the
+  // (1, .5, .25) ellipsoid, kernel 321).  FP64 coordinates relative to the
+  // leaf centre hold it to 2^-53; every other pass keeps the
+  // well-separated, FP32-safe evaluations.
+  bool near64 = false;
+  P2PArgs<double> a64;
+  List near_u;
+  double *sden64 = nullptr, *tval64 = nullptr;
   M2LGeom geom;
   GemmScale scl;
   // device buffers
@@ -105,7 +117,12 @@ struct Impl : ImplBase {
   T* khat;
   T* ktiles = nullptr;  // [td][sd][ceil(nf/32)][343][32] operator spectra for the parent-pair sweep
   T* ttiles = nullptr;  // [td][sd][ceil(nf/16)][26][27][16] Toeplitz-factored operator
-  float* htc_img = nullptr;         // tensor-core Hadamard: operator images per (4 frequencies, direction)
+  float* htc_img = nullptr;         // tensor-core Hadamard (split TF32): operator images per (4 frequencies, direction)
+  unsigned short* htc16_img = nullptr;  // tensor-core Hadamard (FP16 pairs): the same images
+  float* htc16_inv_sb = nullptr;        // ... and the inverse of each chunk's operator scale
+  unsigned* d_bound = nullptr;          // ... and the per-eval bound of the spectra (FP32 bits)
+  int* htc16_ctab = nullptr;            // ... and its colleague tables [tile][26][128]
+  bool htc() const { return htc_img || htc16_img; }
   unsigned* htc_dirs = nullptr;     // tensor-core Hadamard: directions present per tile of 128 parents
   int* h_status = nullptr;  // mapped host word: device-side wait time-outs (bit 0 sweep, bit 1 GEMM, bit 2 TC Hadamard)
   int* d_status = nullptr;
@@ -183,6 +200,31 @@ struct Impl : ImplBase {
     args.tx = upload_as_T(tl[0]);
     args.ty = upload_as_T(tl[1]);
     args.tz = upload_as_T(tl[2]);
+    near64 = sizeof(T) == 4 && E.user.dl;
+    if (near64) {
+      a64.nnodes = nn;
+      a64.ns = E.ns;
+      a64.nt = E.nt;
+      a64.nsurf = nsurf;
+      a64.nuc = nuc;
+      a64.sbeg = args.sbeg;
+      a64.scnt = args.scnt;
+      a64.tbeg = args.tbeg;
+      a64.tcnt = args.tcnt;
+      a64.depth = args.depth;
+      a64.center = args.center;
+      a64.radius = args.radius;
+      a64.sx = upload(sl[0]);
+      a64.sy = upload(sl[1]);
+      a64.sz = upload(sl[2]);
+      a64.snx = upload(sl[3]);
+      a64.sny = upload(sl[4]);
+      a64.snz = upload(sl[5]);
+      a64.tx = upload(tl[0]);
+      a64.ty = upload(tl[1]);
+      a64.tz = upload(tl[2]);
+      a64.l2t_depth = 1 << 30;  // near field only
+    }
     // ---- surfaces and operators
     args.ue_unit = upload_as_T(op.ue);
     args.uc_unit = upload_as_T(op.uc);
@@ -209,7 +251,14 @@ struct Impl : ImplBase {
                 kt[dst] = kh[src];
                 kt[dst + 1] = kh[src + 1];
               }
-        if (sizeof(T) == 4 && E.m2l_tc && m2l_tc_supported(nf, sd_m, td_m)) {
+        if (sizeof(T) == 4 && E.m2l_tc && !E.m2l_tc_tf32 && m2l_tc16_supported(nf, sd_m, td_m)) {
+          std::vector<unsigned short> im;
+          std::vector<float> isb;
+          m2l_tc16_images(nf, op.m2l.data(), &im, &isb);
+          htc16_img = upload(im);
+          htc16_inv_sb = upload(isb);
+          d_bound = dalloc<unsigned>(1);
+        } else if (sizeof(T) == 4 && E.m2l_tc && m2l_tc_supported(nf, sd_m, td_m)) {
           std::vector<float> im;
           m2l_tc_images(nf, op.m2l.data(), &im);
           htc_img = upload(im);
@@ -226,8 +275,10 @@ struct Impl : ImplBase {
     double kc[3];
     kernel_constants(E.user.kt, E.user.coefs, kc);
     args.ku = KConst<T>{(T)kc[0], (T)kc[1], (T)kc[2]};
+    if (near64) a64.ku = KConst<double>{kc[0], kc[1], kc[2]};
     kernel_constants(E.mm.kt, E.mm.coefs, kc);
     args.km = KConst<T>{(T)kc[0], (T)kc[1], (T)kc[2]};
+    if (near64) a64.km = KConst<double>{kc[0], kc[1], kc[2]};
     // ---- per-node data
     supeden = dalloc<T>((size_t)nn * nsurf * sd_m);
     KCHECK(cudaMemset(supeden, 0, sizeof(T) * (size_t)nn * nsurf * sd_m));  // empty nodes stay zero
@@ -317,24 +368,24 @@ struct Impl : ImplBase {
         if (mark[g]) fwdn.push_back(g);
       m2l = make_list(work, {}, ptr, idx);
       fwd = make_list(fwdn, {});
-      effval = dalloc<T>((size_t)nn * td_m * op.nfc * 2);
+      effval = dalloc<T>((size_t)((nn + 15) / 8 * 8) * td_m * op.nfc * 2);  // room for the sibling-group layout
       // nn + 8 blocks: nodes outside every V list keep a zero spectrum, and the
       // 8 blocks from index nn on stand for an absent colleague (parent-pair form)
       // (tensor-core form: sibling-group major, node n in group (n + 7) / 8,
       // the zero block a group of its own: (nn + 15) / 8 groups of 8 nodes)
-      const size_t spec_len = std::max((size_t)(nn + 8) * sd_m, htc_img ? (size_t)(nn + 15) / 8 * 8 : 0) * op.nfc * 2;
+      const size_t spec_len = std::max((size_t)(nn + 8) * sd_m, htc() ? (size_t)(nn + 15) / 8 * 8 : 0) * op.nfc * 2;
       spectra = dalloc<T>(spec_len);
       KCHECK(cudaMemset(spectra, 0, sizeof(T) * spec_len));
       counters_v = (double)idx.size();
-      if (ktiles || ttiles || htc_img) build_pairs(work);
+      if (ktiles || ttiles || htc()) build_pairs(work);
       counters_fwd = (double)fwdn.size();
       counters_inv = (double)work.size();
     }
     // X list (S2L when not direct), leaf work (U + direct W/X; M2T W)
     {
       std::vector<int> xw, lw;
-      std::vector<int64_t> xptr{0}, nptr{0}, mptr{0};
-      std::vector<int> xidx, nidx, midx;
+      std::vector<int64_t> xptr{0}, nptr{0}, mptr{0}, uptr{0};
+      std::vector<int> xidx, nidx, midx, uidx;
       const Csr& U = tr.lists[0];
       const Csr& W = tr.lists[2];
       const Csr& X = tr.lists[3];
@@ -353,7 +404,11 @@ struct Impl : ImplBase {
         }
         if (!term) continue;
         lw.push_back(g);
-        for (int64_t k = U.ptr[g]; k < U.ptr[g + 1]; k++) nidx.push_back(U.idx[k]);
+        for (int64_t k = U.ptr[g]; k < U.ptr[g + 1]; k++) {
+          (near64 ? uidx : nidx).push_back(U.idx[k]);
+          near_int += (double)tr.tcnt[g] * tr.scnt[U.idx[k]] * (near64 ? 1 : 0);
+        }
+        uptr.push_back((int64_t)uidx.size());
         for (int64_t k = W.ptr[g]; k < W.ptr[g + 1]; k++) {
           int w = W.idx[k];
           bool w_direct = tr.terminal(w) && (int64_t)tr.scnt[w] * sd_u < (int64_t)nsurf * sd_m;  // :161
@@ -371,6 +426,7 @@ struct Impl : ImplBase {
       }
       s2l = make_list(xw, {}, xptr, xidx);
       leaf = make_list(lw, {}, nptr, nidx, mptr, midx);
+      if (near64) near_u = make_list(lw, {}, uptr, uidx, std::vector<int64_t>(lw.size() + 1, 0), {});
       for (int g : v_s2m) surf_int += (double)nuc * tr.scnt[g];
       counters_near = near_int;
       counters_surf = surf_int;
@@ -389,7 +445,9 @@ struct Impl : ImplBase {
     geom.td = td_m;
     for (int s = 0; s < sd_m && s < 4; s++) geom.deg[s] = op.deg[s];
     geom.rootlvl = E.rootlvl;
-    geom.sg = htc_img ? 1 : 0;
+    geom.sg = htc16_img ? 2 : htc_img ? 1 : 0;
+    geom.effval_sg = htc16_img ? 1 : 0;
+    geom.bound = d_bound;
     scl.sd = sd_m;
     for (int s = 0; s < sd_m && s < 4; s++) scl.deg[s] = op.deg[s];
     // GEMM flops per eval
@@ -537,7 +595,7 @@ struct Impl : ImplBase {
     pairs_coll = upload(coll);
     pairs_mask = upload(mask);
     pairs_n = (int)qlist.size();
-    if (htc_img) {  // directions present per tile of 128 target parents (an empty tile keeps one)
+    if (htc()) {  // directions present per tile of 128 target parents (an empty tile keeps one)
       std::vector<unsigned> dirs((pairs_n + 127) / 128, 0u);
       double steps = 0;
       for (int t = 0; t < (int)dirs.size(); t++) {
@@ -551,6 +609,11 @@ struct Impl : ImplBase {
       // 128 x 32 x 8 and 8 of 128 x 16 x 8
       counters_tc_had = steps * (op.nfc / 4) * (8.0 * 2 * 128 * 32 * 8 + 8.0 * 2 * 128 * 16 * 8);
       htc_dirs = upload(dirs);
+      if (htc16_img) {
+        std::vector<int> ct;
+        m2l_tc16_tables(pairs_n, tr.nnodes, coll.data(), &ct);
+        htc16_ctab = upload(ct);
+      }
     }
   }
 
@@ -582,6 +645,12 @@ struct Impl : ImplBase {
     cap_rhs = nrhs;
     args.sden = sden;
     args.tval = tval;
+    if (near64) {
+      sden64 = dalloc<double>((size_t)nrhs * E.ns * sd_u);
+      tval64 = dalloc<double>((size_t)nrhs * E.nt * td_u);
+      a64.sden = sden64;
+      a64.tval = tval64;
+    }
   }
 
   // col_lvl set: output rows scaled by 2^(-(depth + rootlvl) * deg)
@@ -624,6 +693,10 @@ struct Impl : ImplBase {
     if (prof) KCHECK(cudaEventRecord(ev[0], st));
     launch_scatter_den<T>(d_srcden, d_sperm, E.ns, sd_u, nrhs, sden, st);
     nlaunch++;
+    if (near64) {
+      launch_scatter_den<double>(d_srcden, d_sperm, E.ns, sd_u, nrhs, sden64, st);
+      nlaunch++;
+    }
     for (int r = 0; r < nrhs; r++) {
       // upward
       p2p(s2m, P2P_S2M, r, st);
@@ -639,9 +712,20 @@ struct Impl : ImplBase {
       // V list
       KCHECK(cudaMemsetAsync(tdncval, 0, sizeof(T) * (size_t)tr.nnodes * nsurf * td_m, st));
       if (m2l.n > 0) {
+        if constexpr (sizeof(T) == 4) {
+          if (htc16_img) {  // the largest value a spectrum can hold, for the FP16 scale
+            launch_spectra_bound(supeden, fwd.work, fwd.n, d_depth, E.rootlvl, op.deg[0], nsurf, d_bound, num_sms, st);
+            nlaunch++;
+          }
+        }
         launch_m2l_forward<T>(geom, supeden, fwd.work, fwd.n, d_depth, spectra, st);
         if (prof && r == 0) KCHECK(cudaEventRecord(ev[7], st));
-        if (pairs_n > 0 && htc_img) {
+        if (pairs_n > 0 && htc16_img) {
+          launch_m2l_hadamard_tc16(E.had_groups, op.nfc, htc16_img, reinterpret_cast<const unsigned*>(spectra),
+                                   pairs_n, pairs_chd, htc16_ctab, htc_dirs, reinterpret_cast<float*>(effval), d_bound,
+                                   htc16_inv_sb, E.wait_limit, d_status, num_sms, st);
+          KCHECK(cudaGetLastError());
+        } else if (pairs_n > 0 && htc_img) {
           launch_m2l_hadamard_tc(op.nfc, htc_img, reinterpret_cast<const float*>(spectra), pairs_n, pairs_chd,
                                  pairs_coll, pairs_mask, htc_dirs, reinterpret_cast<float*>(effval), tr.nnodes,
                                  d_status, num_sms, st);
@@ -676,9 +760,27 @@ struct Impl : ImplBase {
       if (prof && r == 0) KCHECK(cudaEventRecord(ev[4], st));
       // leaves
       p2p(leaf, P2P_LEAF, r, st);
+      if (near64 && near_u.n > 0) {
+        P2PWork w;
+        w.work = near_u.work;
+        w.n = near_u.n;
+        w.ptr = near_u.ptr;
+        w.idx = near_u.idx;
+        w.ptr2 = near_u.ptr2;
+        w.idx2 = near_u.idx2;
+        launch_p2p<double>(E.user.kt, a64, w, P2P_LEAF, r, st);
+        nlaunch++;
+      }
       if (prof && r == 0) KCHECK(cudaEventRecord(ev[5], st));
     }
-    launch_gather_val<T>(tval, d_tperm, E.nt, td_u, nrhs, d_trgval, st);
+    if constexpr (sizeof(T) == 4) {
+      if (near64)
+        launch_gather_val_sum(tval, tval64, d_tperm, E.nt, td_u, nrhs, d_trgval, st);
+      else
+        launch_gather_val<T>(tval, d_tperm, E.nt, td_u, nrhs, d_trgval, st);
+    } else {
+      launch_gather_val<T>(tval, d_tperm, E.nt, td_u, nrhs, d_trgval, st);
+    }
     nlaunch++;
     if (prof) {
       KCHECK(cudaEventRecord(ev[6], st));
@@ -804,6 +906,19 @@ int Engine::setup() {
     // with ~40 % fewer multiply-adds); the direct form in FP64 (faster there)
     m2l_toeplitz = mixed;
     m2l_tc = mixed && tensor_cores;
+    m2l_tc_tf32 = false;
+    int wl = 1 << 22;
+    if (!parse_int(opts, "-" + prefix + "wait_limit", &wl, &found) || wl < 1) {
+      err = "wait_limit must be a positive integer";
+      return KIFMM_ERR_OPTION;
+    }
+    wait_limit = wl;
+    int hg = 3;
+    if (!parse_int(opts, "-" + prefix + "had_groups", &hg, &found) || hg < 2 || hg > 3) {
+      err = "had_groups must be 2 or 3";
+      return KIFMM_ERR_OPTION;
+    }
+    had_groups = hg;
     if (fit != opts.end()) {
       std::string v = fit->second;
       v.erase(0, v.find_first_not_of(" \t"));
@@ -816,8 +931,11 @@ int Engine::setup() {
         m2l_tc = false;
       } else if (v == "tensor") {  // where unsupported (FP64, several dofs): the default form
         m2l_tc = true;
+      } else if (v == "tensor_tf32") {
+        m2l_tc = true;
+        m2l_tc_tf32 = true;
       } else {
-        err = "m2l_form must be tensor, toeplitz or direct";
+        err = "m2l_form must be tensor, tensor_tf32, toeplitz or direct";
         return KIFMM_ERR_OPTION;
       }
     }

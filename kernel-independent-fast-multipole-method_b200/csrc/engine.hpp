@@ -41,7 +41,10 @@ struct Engine {
   bool mixed = false;
   bool tensor_cores = true;  // mixed mode: surface contractions on tcgen05 (split TF32)
   bool m2l_toeplitz = false;  // V-list Hadamard in the 2x2x2 block-Toeplitz factored form
-  bool m2l_tc = false;        // mixed, single-dof kernels: V-list Hadamard on tcgen05 (split TF32)
+  bool m2l_tc = false;        // mixed, single-dof kernels: V-list Hadamard on tcgen05
+  bool m2l_tc_tf32 = false;   // ... with split-TF32 operands instead of FP16 pairs
+  int wait_limit = 1 << 22;   // polls before a device-side pipeline wait gives up (-<prefix>wait_limit)
+  int had_groups = 3;         // producer groups of the FP16 tensor-core Hadamard (-<prefix>had_groups)
   bool profiling = false;
   // state
   bool ready = false;       // device state built, eval allowed

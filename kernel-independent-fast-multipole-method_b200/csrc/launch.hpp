@@ -31,6 +31,10 @@ struct P2PArgs {
   T* supcval = nullptr;
   T* tdncval = nullptr;
   KConst<T> ku{}, km{};  // user and equivalent kernel constants
+  // leaves at this depth and below add L2T from their downward equivalent
+  // surface in the leaf pass (a pass with near-field sources only sets it
+  // beyond the deepest level)
+  int l2t_depth = 2;
 };
 
 enum { P2P_S2M = 0, P2P_S2L = 1, P2P_LEAF = 2 };
@@ -54,6 +58,9 @@ template <typename T>
 void launch_scatter_den(const double* srcden, const int* perm, int ns, int sd, int nrhs, T* out, cudaStream_t st);
 template <typename T>
 void launch_gather_val(const T* tval, const int* perm, int nt, int td, int nrhs, double* trgval, cudaStream_t st);
+// the same gather of tval + near (an FP64 near-field sum beside FP32 passes)
+void launch_gather_val_sum(const float* tval, const double* near, const int* perm, int nt, int td, int nrhs,
+                           double* trgval, cudaStream_t st);
 
 // Batched node GEMM: for j < ncol,
 //   C[cidx[j]*ldc + r] (=|+=) rs(j, r) * sum_k A[r*K + k] * B[bidx[j]*ldb + k]
@@ -113,11 +120,22 @@ struct M2LGeom {
   int sd = 1, td = 1;
   int deg[4] = {0, 0, 0, 0};
   int rootlvl = 0;
+  // 2: the sibling-group-major layout holding FP16 pairs (below)
   // 0: spectra[node][s][f]; 1 (single dof): sibling-group major,
   // spectra[(node + 7) / 8][f / 4][(node + 7) % 8][f % 4] -- every sibling
   // group's spectra one block, and in it the 8 children's values of 4
   // frequencies 256 contiguous bytes (first children are 1 mod 8)
   int sg = 0;
+  // sg == 2: each complex value x is stored as the FP16 pairs
+  // {hi(re), hi(im)}, {lo(re), lo(im)} of x * 2^(14 - e), where 2^e >= the
+  // FP32 value *bound (k_spectra_bound) -- the operands of the 16-bit
+  // tensor-core Hadamard, in the 8 bytes (spectra_sg_index) the FP32 value
+  // would take
+  const unsigned* bound = nullptr;
+  // accumulated spectra (single dof) in the sibling-group-major layout of
+  // spectra_sg_index instead of [node][td][nfc] (written so by the FP16
+  // tensor-core Hadamard)
+  int effval_sg = 0;
 };
 // complex index of (node, compact frequency c) in the sibling-group-major
 // layout of nfc frequencies (a multiple of 4)
@@ -166,6 +184,27 @@ void m2l_tc_images(int nf, const std::complex<double>* m2l, std::vector<float>* 
 void launch_m2l_hadamard_tc(int nf, const float* img, const float* spectra, int nq, const int* qchd,
                             const int* coll, const unsigned char* mask, const unsigned* tile_dirs, float* effval,
                             int zero_node, int* status, int num_sms, cudaStream_t st);
+// The same product on the tensor cores with FP16-pair operands (kind::f16,
+// m2l_tc16.cu): spectra written by the forward pass in the sg == 2 layout
+// (scaled by the data bound *bound), img per (chunk of 4 frequencies,
+// direction) the hi and lo FP16 images of the 16 x 16 real blocks, scaled by
+// 1 / inv_sb[chunk] (m2l_tc16_images).  groups: producer warp groups = TMEM A
+// stages (2 or 3 groups: 4 or 6 stages).  wait_limit bounds every pipeline
+// wait (polls); a time-out sets bit 3 of *status.
+bool m2l_tc16_supported(int nf, int sd, int td);
+void m2l_tc16_images(int nf, const std::complex<double>* m2l, std::vector<unsigned short>* img,
+                     std::vector<float>* inv_sb);
+// *bound = max over nodes of 2^((depth + rootlvl) deg) * sum |supeden[node]| (one dof, FP32 bits)
+void launch_spectra_bound(const float* supeden, const int* nodes, int n, const int* depth, int rootlvl, int deg,
+                          int nsurf, unsigned* bound, int num_sms, cudaStream_t st);
+void launch_m2l_hadamard_tc16(int groups, int nf, const unsigned short* img, const unsigned* spectra, int nq,
+                              const int* qchd, const int* ctab, const unsigned* tile_dirs, float* effval,
+                              const unsigned* bound, const float* inv_sb, int wait_limit, int* status, int num_sms,
+                              cudaStream_t st);
+// colleague tables of the FP16 form: per tile of 128 target parents and
+// direction, the sibling group ((first child + 7) / 8) of each row's colleague
+// (the all-zero group for an absent one or a padding row), [tile][26][128]
+void m2l_tc16_tables(int nq, int zero_node, const int* coll, std::vector<int>* ctab);
 // tdncval[node] += extract(inverse(effval[node]))
 template <typename T>
 void launch_m2l_inverse(const M2LGeom& g, const T* effval, const int* work, int nwork, T* tdncval,

@@ -20,6 +20,8 @@
 // reads back (conjugating the mirrored half) only the independent values.
 // Density and potential grids use indices [0, np) per axis; the reference's
 // np/2 shift (matmgnt3d.cpp:256) cancels between embedding and extraction.
+#include <cuda_fp16.h>
+
 #include <algorithm>
 
 #include "launch.hpp"
@@ -370,6 +372,25 @@ __device__ __forceinline__ T twi(int m) {
     return c_twd_im[t][m % N];
 }
 
+// scale 2^(14 - e) of the FP16-pair spectra, 2^e >= the bound (1 without one)
+__device__ __forceinline__ float spectra_scale16(const unsigned* bound) {
+  const float b = bound ? __uint_as_float(*bound) : 0.f;
+  if (!(b > 0.f)) return 1.f;
+  int e;
+  frexpf(b, &e);
+  return ldexpf(1.f, 14 - e);
+}
+
+// x * s as {hi(re), hi(im)}, {lo(re), lo(im)}: FP16 rounded to nearest,
+// lo = the FP16 rounding of what hi leaves over
+__device__ __forceinline__ uint2 f16_pairs(float re, float im, float s) {
+  const float xr = re * s, xi = im * s;
+  const __half2 hi = __floats2half2_rn(xr, xi);
+  const float2 hf = __half22float2(hi);
+  const __half2 lo = __floats2half2_rn(xr - hf.x, xi - hf.y);
+  return make_uint2(*reinterpret_cast<const unsigned*>(&hi), *reinterpret_cast<const unsigned*>(&lo));
+}
+
 template <typename T, int NP>
 __global__ void __launch_bounds__(256) k_m2l_fwd_rb(M2LGeom g, const T* __restrict__ supeden,
                                                     const int* __restrict__ nodes, int nwork,
@@ -387,6 +408,7 @@ __global__ void __launch_bounds__(256) k_m2l_fwd_rb(M2LGeom g, const T* __restri
   // __syncwarp separates from the y pass's first write of Bm
   T* xg = reinterpret_cast<T*>(Bm);
   static_assert(sizeof(T) * NP * NP * NP <= sizeof(Cpx<T>) * NP * N * NH, "density grid fits in Bm");
+  const float s16 = g.sg == 2 ? spectra_scale16(g.bound) : 1.f;
   __syncthreads();
   for (int wi = blockIdx.x * wpc + warp; wi < nwork; wi += gridDim.x * wpc) {
     const int node = nodes[wi];
@@ -456,6 +478,12 @@ __global__ void __launch_bounds__(256) k_m2l_fwd_rb(M2LGeom g, const T* __restri
             re = fmt(-b[k].im, ci, fmt(b[k].re, cr, re));
             im = fmt(b[k].im, cr, fmt(b[k].re, ci, im));
           }
+          if constexpr (sizeof(T) == 4) {
+            if (g.sg == 2) {
+              reinterpret_cast<uint2*>(spectra)[spectra_sg_index(NFC, node, c)] = f16_pairs(re, im, s16);
+              continue;
+            }
+          }
           if (g.sg)
             reinterpret_cast<Cpx<T>*>(spectra)[spectra_sg_index(NFC, node, c)] = Cpx<T>{re, im};
           else
@@ -492,6 +520,8 @@ __global__ void __launch_bounds__(256) k_m2l_inv_rb(M2LGeom g, const T* __restri
     T* dst = tdncval + (size_t)node * NSURF * g.td;
     for (int t = 0; t < g.td; t++) {
       const Cpx<T>* src = reinterpret_cast<const Cpx<T>*>(effval + ((size_t)node * g.td + t) * NFC * 2);
+      // sibling-group-major accumulated spectra (single dof): value c at spectra_sg_index
+      const Cpx<T>* srcg = reinterpret_cast<const Cpx<T>*>(effval) + spectra_sg_index(NFC, node, 0);
       // z pass (inverse), lines (ky, kx): Bm[k][ky][kx] = sum_kz Y[kz][ky][kx] w^(-k kz), k < np
       for (int line = lane; line < N * NH; line += 32) {
         const int kx = line % NH, ky = line / NH;
@@ -499,7 +529,8 @@ __global__ void __launch_bounds__(256) k_m2l_inv_rb(M2LGeom g, const T* __restri
 #pragma unroll
         for (int kz = 0; kz < N; kz++) {
           const int c = c_of[(kz * N + ky) * NH + kx];
-          Cpx<T> v = src[c >= 0 ? c : -c - 1];
+          const int ca = c >= 0 ? c : -c - 1;
+          Cpx<T> v = g.effval_sg ? srcg[(ca >> 2) * 32 + (ca & 3)] : src[ca];
           if (c < 0) v.im = -v.im;
           y[kz] = v;
         }

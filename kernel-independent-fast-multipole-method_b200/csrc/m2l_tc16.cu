@@ -1,0 +1,622 @@
+// V-list Hadamard accumulate on the 5th-generation tensor cores with 16-bit
+// operands (tcgen05, kind::f16) for single-dof equivalent kernels in mixed
+// precision: the frequency-domain product of the reference's M2L
+// (fmm3d/fmm3d_eval.cpp:115-150, MatMgnt3d::UE2DC_dgemv
+// fmm3d/matmgnt3d.cpp:272-290), in the parent-pair form of the V list.
+//
+// For target parent Q, colleague direction d (P = Q + d) and frequency f the
+// V-list products of Q's 8 children with P's 8 children are one 8 x 8
+// complex block, M[i][j] = K(2d + oct(j) - oct(i)) (zero for adjacent child
+// pairs), applied to P's 8 child spectra; in real arithmetic a 16 x 16
+// block B_d(f), and for a tile of 128 target parents
+//   D(f)[128 x 16] = sum_d A_d(f)[128 x 16] B_d(f)^T,
+// A_d(f) row q = the 8 child spectra of q's colleague in direction d.
+//
+// Operands are FP16 pairs: every spectrum value x (scaled by a power of two
+// s_A) is stored as hi = fp16(x s_A) and lo = fp16(x s_A - hi), both rounded
+// to nearest, so hi + lo carries x to 2^-22; the operator images likewise
+// with a per-chunk power-of-two scale s_B.  Per frequency two MMAs
+//   D[0:32)  += A_hi [B_hi | B_lo]^T    (N = 32)
+//   D[0:16)  += A_lo B_hi^T             (N = 16)
+// and the drain adds D[16:32) to D[0:16) and multiplies by 1/(s_A s_B):
+// head*head, both cross terms, lo*lo (2^-22 relative) dropped, the products
+// exact in the FP32 accumulator.  s_A = 2^(14 - e) with 2^e >= the largest
+// |x| any spectrum can hold (the L1 norm of a node's scaled density grid,
+// reduced over the nodes by k_spectra_bound before the forward transform), so
+// |hi| <= 2^14 never overflows FP16; values more than 2^28 below the bound
+// lose precision, i.e. none that matter against the accumulated sum.
+//
+// The forward transform writes the pairs already split, in the 8 bytes an
+// FP32 complex value takes in the sibling-group-major layout (the 8 children
+// of a colleague x 4 frequencies x {hi, lo} x {re, im} = 256 contiguous
+// bytes, 32 per child), so a producer only moves bytes: four adjacent
+// threads read one row's 128-byte line (children 0-3, then 4-7) with 32-byte
+// loads, and the K order of the A rows (column 2c + e of a column block =
+// child c + 4e, the operator images permuted to match) lets thread c write
+// what it loaded with 16x256b TMEM stores.  Against the TF32 form this halves
+// the TMEM bytes per step (32 KB), the A stage (64 columns, so six stages fit
+// beside the 128-column accumulator instead of three) and the operator
+// images (4 KB per step), removes the producers' split arithmetic, and runs
+// the MMAs at the 16-bit rate.
+//
+// Work items are (frequency chunk of 4, tile of 128 target parents), chunk
+// major over a persistent grid; inside an item the steps are the tile's
+// present colleague directions.  Warp roles, handing over through mbarriers:
+//   warps 0 .. 4G-1  producers, G groups of four (one warp per TMEM lane
+//               quarter); group g fills the steps s = g mod G, step s into A
+//               stage s mod 2G, so a group's stage wait looks two of its own
+//               steps back.  Per step a producer thread issues all eight of
+//               its 32-byte loads at once (the step waits for memory once),
+//               reads the colleague groups of its rows at the group's next
+//               step from the tile-major colleague table (m2l_tc16_tables)
+//               right after them, and issues the step's operator-image copy
+//               (image stage s mod 3G) before waiting for its A stage.
+//   warps 4G .. 4G+3  MMA warps: warp 4G + f issues frequency f's 2 MMAs of
+//               every step (own accumulator columns, one elected lane) and
+//               commits; at an item's end each drains TMEM lane quarter
+//               (warp mod 4), all four frequencies, into the
+//               sibling-group-major accumulated spectra with 32-byte stores
+//               (a target parent's 8 children x 4 frequencies are one block)
+//   bfull[3G]  (bytes)         operator images landed           copy -> producers
+//   afull[2G]  (128 arrivals)  A stage written, images landed   producers -> MMA
+//   aempty[2G] (4 commits)     step's MMAs done                 MMA -> producers
+//   accfull    (4 commits)     item's MMAs done                 MMA -> drain
+//   accempty   (128 arrivals)  accumulator read out             drain -> MMA
+// Every pipeline wait is bounded by wait_limit polls; a time-out sets bit 3
+// of *status and ends the CTA after its copies landed and its MMAs completed
+// (those two final waits use a fixed, long bound).
+#include <cuda_fp16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <vector>
+
+#include "launch.hpp"
+
+namespace kifmm {
+namespace {
+
+constexpr int H16_M = 128;                       // target parents per tile (MMA M, TMEM lanes)
+constexpr int H16_F = 4;                         // frequencies per item
+// G producer groups (2 or 3), 2 G A stages (128 + 128 G TMEM columns), MMA
+// warps from warp 4 G on, 3 G operator image stages
+constexpr int h16_threads(int G) { return (4 * G + 4) * 32; }
+constexpr unsigned H16_IMG_BYTES = H16_F * 1024;  // per (chunk, direction): F x [32 rows x 16 K] fp16
+constexpr unsigned H16_COLS = 512;               // accumulator 0-127, A stages 128-511
+constexpr unsigned H16_ACOL0 = H16_F * 32;
+constexpr unsigned H16_ACOLS = 64;               // TMEM columns per A stage
+constexpr int H16_LONG_WAIT = 1 << 22;           // polls of the end-of-CTA waits
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned parity, int limit) {
+  for (int it = 0; it < limit; it++) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
+// non-blocking test of an mbarrier phase
+__device__ __forceinline__ bool mbar_test(unsigned bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ void bulk_load(unsigned dst, const void* src, unsigned bytes, unsigned bar) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+
+// no-swizzle K-major descriptor of one frequency's operator image (32 rows x
+// 16 K of fp16): the two K-adjacent core matrices 512 B apart (LBO), row
+// groups of 8 128 B apart (SBO)
+__device__ __forceinline__ uint64_t img_desc16(unsigned addr) {
+  const uint64_t lbo = 512, sbo = 128;
+  return (uint64_t)((addr & 0x3FFFFu) >> 4) | ((lbo >> 4) << 16) | ((sbo >> 4) << 32) | (1ull << 46);
+}
+
+// kind::f16, D F32, A and B FP16, both K-major, M = 128
+template <int N>
+__device__ __forceinline__ constexpr unsigned idesc_f16() {
+  return (1u << 4) | ((unsigned)(N >> 3) << 17) | ((unsigned)(H16_M >> 4) << 24);
+}
+
+// one frequency's 2 MMAs of a step, issued by one elected lane of the
+// converged warp: D[d, +32) (+)= A_hi [B_hi | B_lo]^T, D[d, +16) += A_lo B_hi^T
+// (A_lo 8 columns after A_hi); the first product overwrites D when acc == 0
+__device__ __forceinline__ void mma_freq16(unsigned d, unsigned a, uint64_t b, int acc) {
+  asm volatile(
+      "{\n"
+      " .reg .pred e, p, t;\n"
+      " .reg .b32 a;\n"
+      " setp.ne.b32 p, %3, 0;\n"
+      " setp.eq.b32 t, %3, %3;\n"
+      " elect.sync _|e, 0xffffffff;\n"
+      " @e tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %4, p;\n"
+      " add.u32 a, %1, 8;\n"
+      " @e tcgen05.mma.cta_group::1.kind::f16 [%0], [a], %2, %5, t;\n"
+      "}\n" ::"r"(d),
+      "r"(a), "l"(b), "r"(acc), "r"(idesc_f16<32>()), "r"(idesc_f16<16>())
+      : "memory");
+}
+
+__device__ __forceinline__ void commit_elect(unsigned bar) {
+  asm volatile(
+      "{\n .reg .pred e;\n elect.sync _|e, 0xffffffff;\n"
+      " @e tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n}\n" ::"r"(bar)
+      : "memory");
+}
+
+// 16 TMEM lanes x 32 columns: registers 4 i .. 4 i + 3 go to column block i
+// (8 columns); thread t's registers 4 i, 4 i + 1 to lane t / 4, columns
+// 8 i + 2 (t % 4) + {0, 1}, registers 4 i + 2, 4 i + 3 to lane t / 4 + 8
+__device__ __forceinline__ void tmem_st16x256_x4(unsigned taddr, const unsigned* r) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.16x256b.x4.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(
+          taddr),
+      "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]),
+      "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15])
+      : "memory");
+}
+
+// one 32-byte read-only load
+__device__ __forceinline__ void ld32B(const unsigned* p, unsigned* r) {
+  asm volatile("ld.global.nc.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+               : "l"(p));
+}
+
+// one 32-byte store
+__device__ __forceinline__ void st32B(float* p, float a, float b, float c, float d, float e, float f, float g, float h) {
+  asm volatile("st.global.v8.f32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(p), "f"(a), "f"(b), "f"(c), "f"(d), "f"(e),
+               "f"(f), "f"(g), "f"(h)
+               : "memory");
+}
+
+// 16 consecutive columns of this thread's TMEM lane
+__device__ __forceinline__ void tmem_ld16(unsigned taddr, unsigned* r) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+}
+
+// 2^(e - 14) for the data bound b <= 2^e (b > 0), the inverse of the data scale
+__device__ __forceinline__ float inv_data_scale(float b) {
+  if (!(b > 0.f)) return 1.f;
+  int e;
+  frexpf(b, &e);
+  return ldexpf(1.f, e - 14);
+}
+
+constexpr int H16_NBI = 9;  // room for the operator image stages (G + 2 G for G <= 3)
+
+// dynamic shared memory: image stages, then the CTA's item direction masks
+constexpr size_t h16_smem(int max_items) { return (size_t)H16_NBI * H16_IMG_BYTES + 4 * (size_t)max_items; }
+
+// one step forward in a CTA's step sequence (items li in grid-stride order,
+// the directions d of each item's mask dm); false past the last item
+__device__ __forceinline__ bool h16_step(int& li, int& d, int& fc, int& tile, unsigned& dm, const unsigned* dirs,
+                                         int my_items, int ntiles) {
+  const unsigned rest = d >= 25 ? 0u : (dm >> (d + 1));
+  if (rest) {
+    d += __ffs(rest);
+    return true;
+  }
+  if (++li >= my_items) return false;
+  tile += gridDim.x;
+  while (tile >= ntiles) {
+    tile -= ntiles;
+    fc++;
+  }
+  dm = dirs[li];
+  d = __ffs(dm) - 1;
+  return true;
+}
+
+// G steps forward: inside an item the G-th set bit of the mask above d,
+// across an item's end single steps
+template <int G>
+__device__ __forceinline__ bool h16_stepG(int& li, int& d, int& fc, int& tile, unsigned& dm, const unsigned* dirs,
+                                          int my_items, int ntiles) {
+  if (d < 25) {
+    unsigned r = dm >> (d + 1);
+#pragma unroll
+    for (int k = 0; k < G - 1; k++) r &= r - 1u;
+    if (r) {
+      d += __ffs(r);
+      return true;
+    }
+  }
+  bool ok = true;
+#pragma unroll 1
+  for (int k = 0; k < G && ok; k++) ok = h16_step(li, d, fc, tile, dm, dirs, my_items, ntiles);
+  return ok;
+}
+
+template <int NF, int H16_G>
+__global__ void __launch_bounds__(h16_threads(H16_G), 1)
+    k_m2l_had_tc16(const unsigned char* __restrict__ img, const unsigned* __restrict__ spectra, int nq, int ntiles,
+                   const int* __restrict__ qchd, const int* __restrict__ ctab, const unsigned* __restrict__ tile_dirs,
+                   float* __restrict__ effval, int nitems, const unsigned* __restrict__ bound,
+                   const float* __restrict__ inv_sb, int wait_limit, int* __restrict__ status) {
+  constexpr int H16_MMA_WARP = H16_G * 4;  // first of the 4 MMA warps
+  constexpr int H16_S = 2 * H16_G;         // A stages: step s uses stage s mod S
+  constexpr int H16_NB = H16_G + H16_S;    // operator image stages: step s uses s mod NB
+  static_assert(H16_ACOL0 + H16_S * H16_ACOLS <= H16_COLS, "A stages fit in TMEM");
+  static_assert(H16_NB <= H16_NBI, "image stages");
+  extern __shared__ __align__(1024) unsigned char smem[];
+  unsigned char* imgs = smem;                                       // [NB][4 KB]
+  unsigned* dirs = reinterpret_cast<unsigned*>(smem + (size_t)H16_NBI * H16_IMG_BYTES);
+  __shared__ __align__(8) unsigned long long afull[H16_S], aempty[H16_S], bfull[H16_NB], accfull, accempty, lastbar;
+  __shared__ unsigned tmem_base;
+  __shared__ int fail;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if ((int)blockIdx.x >= nitems) return;
+  const int my_items = (nitems - 1 - (int)blockIdx.x) / (int)gridDim.x + 1;
+  auto tile_of = [&](int li) {
+    const int i = blockIdx.x + li * gridDim.x;
+    return i - (i / ntiles) * ntiles;
+  };
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
+                 "r"(H16_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    for (int b = 0; b < H16_S; b++) {
+      mbar_init(smem_u32(&afull[b]), 128);
+      mbar_init(smem_u32(&aempty[b]), H16_F);
+    }
+    for (int b = 0; b < H16_NB; b++) mbar_init(smem_u32(&bfull[b]), 1);
+    mbar_init(smem_u32(&accfull), H16_F);
+    mbar_init(smem_u32(&accempty), 128);
+    mbar_init(smem_u32(&lastbar), H16_F);
+    fail = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  for (int li = tid; li < my_items; li += blockDim.x) dirs[li] = __ldg(tile_dirs + tile_of(li));
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const unsigned tmem = tmem_base;
+  volatile int* vfail = &fail;
+  // warp-uniform bounded wait (the tcgen05 .sync.aligned operations after it
+  // need the whole warp): false for every lane once any wait has timed out
+  auto wait = [&](unsigned long long* bar, int parity) {
+    const bool ok = mbar_wait_bounded(smem_u32(bar), parity, wait_limit);
+    if (__all_sync(0xffffffffu, ok)) return true;
+    *vfail = 1;
+    return false;
+  };
+
+  if (warp < H16_MMA_WARP) {
+    // ---- producers: warp (grp, quarter qd) writes TMEM lanes 32 qd .. + 31
+    // in two halves h of 16; thread t carries rows t / 4 and t / 4 + 8 (ab)
+    // of each half and children c, c + 4 (c = t % 4) of each row's colleague
+    const int grp = warp >> 2, qd = warp & 3, c = lane & 3;
+    const int rbase = qd * 32 + (lane >> 2);
+    const unsigned abase = tmem + H16_ACOL0 + ((unsigned)(qd * 32) << 16);
+    // the group's steps s = grp, grp + G, ...: item li, direction d; the
+    // item's chunk fc and tile advance by grid strides
+    int li = 0, d = -1, fc = blockIdx.x / ntiles, tile = blockIdx.x - fc * ntiles;
+    unsigned dm = dirs[0];
+    bool ok = true;
+    for (int k = 0; k <= grp && ok; k++) ok = h16_step(li, d, fc, tile, dm, dirs, my_items, ntiles);
+    // the colleague groups of this thread's 4 rows at the group's next step,
+    // loaded one group step ahead of their use
+    int g0 = 0, g1 = 0, g2 = 0, g3 = 0;
+#define H16_LOAD_G()                                                  \
+  {                                                                   \
+    const int* tb = ctab + ((size_t)tile * 26 + d) * H16_M + rbase;   \
+    g0 = __ldg(tb);                                                   \
+    g1 = __ldg(tb + 8);                                               \
+    g2 = __ldg(tb + 16);                                              \
+    g3 = __ldg(tb + 24);                                              \
+  }
+    if (ok) H16_LOAD_G()
+    int s = grp, pend = -1;  // pend: step of an operator copy not yet seen landed
+    while (ok) {
+      // the step's operator images into stage s mod NB, last read by step
+      // s - NB; this group's stage wait of step s - G saw the MMAs of step
+      // s - G - S complete, and NB = G + S
+      if (qd == 0 && lane == 0)
+        bulk_load(smem_u32(imgs + (size_t)(s % H16_NB) * H16_IMG_BYTES), img + ((size_t)fc * 26 + d) * H16_IMG_BYTES,
+                  H16_IMG_BYTES, smem_u32(&bfull[s % H16_NB]));
+      if (qd == 0) pend = s;
+      // all of the step's loads at once: x[h][ab][e][w] = word w
+      // (frequency w / 2, {hi, lo} = w % 2) of child c + 4 e of the
+      // colleague of row (h, ab), so the step waits for memory once
+      unsigned x[2][2][2][8];
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        const int gk = k == 0 ? g0 : k == 1 ? g1 : k == 2 ? g2 : g3;
+        const unsigned* src = spectra + (((size_t)gk * (NF / H16_F) + fc) * 64) + 8 * c;
+        ld32B(src, x[k >> 1][k & 1][0]);
+        ld32B(src + 32, x[k >> 1][k & 1][1]);
+      }
+      const int stg = s % H16_S, sb = s % H16_NB, sbp = (s / H16_NB) & 1;
+      ok = h16_stepG<H16_G>(li, d, fc, tile, dm, dirs, my_items, ntiles);
+      if (ok) H16_LOAD_G()  // the g's are free once the step's loads are issued
+      if (s >= H16_S && !wait(&aempty[stg], ((s / H16_S) + 1) & 1)) break;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      // column block b = 2 f + {hi, lo}; in every block column 2c + e holds
+      // child c + 4e; one store per half h and pair of frequencies L
+#pragma unroll
+      for (int h = 0; h < 2; h++)
+#pragma unroll
+        for (int L = 0; L < 2; L++) {
+          unsigned r[16];
+#pragma unroll
+          for (int i = 0; i < 4; i++) {
+            r[4 * i + 0] = x[h][0][0][4 * L + i];
+            r[4 * i + 1] = x[h][0][1][4 * L + i];
+            r[4 * i + 2] = x[h][1][0][4 * L + i];
+            r[4 * i + 3] = x[h][1][1][4 * L + i];
+          }
+          tmem_st16x256_x4(abase + (unsigned)stg * H16_ACOLS + ((unsigned)(16 * h) << 16) + 32 * L, r);
+        }
+      asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      if (qd == 0) {
+        if (!wait(&bfull[sb], sbp)) break;
+        pend = -1;
+      }
+      asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&afull[stg])) : "memory");
+      s += H16_G;
+    }
+#undef H16_LOAD_G
+    // after a time-out: the copy this warp issued last has landed before the CTA ends
+    if (pend >= 0) mbar_wait_bounded(smem_u32(&bfull[pend % H16_NB]), (pend / H16_NB) & 1, H16_LONG_WAIT);
+  } else {
+    // ---- MMA warps: warp H16_MMA_WARP + f issues frequency f's 2 MMAs of
+    // every step (own accumulator columns, one elected lane) and commits;
+    // the next step's afull is tested without blocking before this step's
+    // MMAs go out.  At an item's end each drains TMEM lane quarter
+    // (warp mod 4), all four frequencies, into effval.
+    const int f = warp - H16_MMA_WARP;
+    const float inv_sa = inv_data_scale(__uint_as_float(*bound));
+    int s = 0;
+    bool ready = false, failed = false;
+    // A_hi of frequency f: column block 2 f, A_lo block 2 f + 1
+    const unsigned acol = H16_ACOL0 + 16 * f;
+    for (int li = 0; li < my_items; li++) {
+      const int nst = __popc(dirs[li]);
+      for (int k = 0; k < nst; k++) {
+        const int stg = s % H16_S;
+        if (!__all_sync(0xffffffffu, ready) && !wait(&afull[stg], (s / H16_S) & 1)) {
+          failed = true;
+          break;
+        }
+        if (k == 0 && li >= 1 && !wait(&accempty, (li - 1) & 1)) {
+          failed = true;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const int s1 = s + 1;
+        ready = mbar_test(smem_u32(&afull[s1 % H16_S]), (s1 / H16_S) & 1);
+        mma_freq16(tmem + f * 32, tmem + acol + (unsigned)stg * H16_ACOLS,
+                   img_desc16(smem_u32(imgs + (size_t)(s % H16_NB) * H16_IMG_BYTES + f * 1024)), k == 0 ? 0 : 1);
+        commit_elect(smem_u32(&aempty[stg]));
+        s++;
+      }
+      if (failed) break;
+      commit_elect(smem_u32(&accfull));
+      // drain item li from TMEM lane quarter (warp & 3) into effval
+      if (!wait(&accfull, li & 1)) break;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const int i = blockIdx.x + li * gridDim.x;
+      const int fc = i / ntiles, tile = i - fc * ntiles;
+      const int row = (warp & 3) * 32 + lane;
+      const unsigned lane_off = (unsigned)((warp & 3) * 32) << 16;
+      const int q = tile * H16_M + row;
+      const float scl = inv_sa * __ldg(inv_sb + fc);
+      // frequency f2: head*head + tail*head in columns 32 f2 + 0-15,
+      // head*tail in 32 f2 + 16-31; y[f2][2 i + (re, im)] of child i
+      float y[H16_F][16];
+#pragma unroll
+      for (int f2 = 0; f2 < H16_F; f2++) {
+        unsigned r[16];
+        tmem_ld16(tmem + lane_off + f2 * 32, r);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+        for (int n = 0; n < 16; n++) y[f2][n] = __uint_as_float(r[n]);
+        tmem_ld16(tmem + lane_off + f2 * 32 + 16, r);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+        for (int n = 0; n < 16; n++) y[f2][n] = (y[f2][n] + __uint_as_float(r[n])) * scl;
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&accempty)) : "memory");
+      // the row's 8 children x 4 frequencies: one 256-byte block of the
+      // sibling-group-major accumulated spectra (all 8 children; the inverse
+      // pass reads only the V-list targets among them)
+      if (q < nq) {
+        float* dst = effval + (((size_t)((qchd[q] + 7) >> 3) * (NF / H16_F) + fc) * 64);
+#pragma unroll
+        for (int ch = 0; ch < 8; ch++)
+          st32B(dst + 8 * ch, y[0][2 * ch], y[0][2 * ch + 1], y[1][2 * ch], y[1][2 * ch + 1], y[2][2 * ch],
+                y[2][2 * ch + 1], y[3][2 * ch], y[3][2 * ch + 1]);
+      }
+    }
+    // before the CTA ends every MMA issued has completed (only a time-out
+    // leaves any outstanding)
+    commit_elect(smem_u32(&lastbar));
+    mbar_wait_bounded(smem_u32(&lastbar), 0, H16_LONG_WAIT);
+  }
+  __syncthreads();
+  if (*vfail && tid == 0) atomicOr(status, 8);
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(H16_COLS) : "memory");
+  }
+}
+
+// bound = max over the nodes of 2^(lvl deg) * sum |supeden[node]| (one dof),
+// as FP32 bits (non-negative floats order like their bit patterns)
+__global__ void __launch_bounds__(256) k_spectra_bound(const float* __restrict__ supeden, const int* __restrict__ nodes,
+                                                       int n, const int* __restrict__ depth, int rootlvl, int deg,
+                                                       int nsurf, unsigned* __restrict__ bound) {
+  float best = 0.f;
+  const int lane = threadIdx.x & 31;
+  for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < n; w += (gridDim.x * blockDim.x) >> 5) {
+    const int node = nodes[w];
+    const float* u = supeden + (size_t)node * nsurf;
+    float s = 0.f;
+    for (int k = lane; k < nsurf; k += 32) s += fabsf(u[k]);
+#pragma unroll
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    best = fmaxf(best, ldexpf(s, (depth[node] + rootlvl) * deg));
+  }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) best = fmaxf(best, __shfl_xor_sync(0xffffffffu, best, o));
+  __shared__ float red[8];
+  if (lane == 0) red[threadIdx.x >> 5] = best;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float b = 0.f;
+    for (int k = 0; k < (int)(blockDim.x >> 5); k++) b = fmaxf(b, red[k]);
+    // a little headroom for the rounding of the FP32 transform
+    atomicMax(bound, __float_as_uint(b * 1.0001f));
+  }
+}
+
+template <int NF, int G>
+void had_tc16_launch_g(const unsigned char* img, const unsigned* spectra, int nq, const int* qchd, const int* ctab,
+                       const unsigned* tile_dirs, float* effval, const unsigned* bound, const float* inv_sb,
+                       int wait_limit, int* status, int num_sms, cudaStream_t st) {
+  const int ntiles = (nq + H16_M - 1) / H16_M;
+  const int nitems = ntiles * (NF / H16_F);
+  if (nitems == 0) return;
+  const int grid = std::min(num_sms, nitems);
+  const size_t smem = h16_smem((nitems + grid - 1) / grid);
+  auto kern = k_m2l_had_tc16<NF, G>;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  kern<<<grid, h16_threads(G), smem, st>>>(img, spectra, nq, ntiles, qchd, ctab, tile_dirs, effval, nitems, bound,
+                                           inv_sb, wait_limit, status);
+}
+
+template <int NF>
+void had_tc16_launch(int groups, const unsigned char* img, const unsigned* spectra, int nq, const int* qchd,
+                     const int* ctab, const unsigned* tile_dirs, float* effval, const unsigned* bound,
+                     const float* inv_sb, int wait_limit, int* status, int num_sms, cudaStream_t st) {
+  if (groups == 2)
+    had_tc16_launch_g<NF, 2>(img, spectra, nq, qchd, ctab, tile_dirs, effval, bound, inv_sb, wait_limit, status,
+                             num_sms, st);
+  else
+    had_tc16_launch_g<NF, 3>(img, spectra, nq, qchd, ctab, tile_dirs, effval, bound, inv_sb, wait_limit, status,
+                             num_sms, st);
+}
+
+}  // namespace
+
+bool m2l_tc16_supported(int nf, int sd, int td) {
+  return sd == 1 && td == 1 && (nf == 260 || nf == 868 || nf == 2052);
+}
+
+void m2l_tc16_images(int nf, const std::complex<double>* m2l, std::vector<unsigned short>* img,
+                     std::vector<float>* inv_sb) {
+  const int nch = nf / H16_F;
+  img->assign((size_t)nch * 26 * (H16_IMG_BYTES / 2), 0);
+  inv_sb->assign(nch, 1.f);
+  for (int fc = 0; fc < nch; fc++) {
+    // the chunk's scale: 2^(14 - e) with every |entry| <= 2^e
+    double mx = 0;
+    for (int o = 0; o < 343; o++)
+      for (int f = fc * H16_F; f < fc * H16_F + H16_F; f++) {
+        const std::complex<double> t = m2l[(size_t)o * nf + f];
+        mx = std::max(mx, std::max(std::abs(t.real()), std::abs(t.imag())));
+      }
+    int e = 0;
+    if (mx > 0) std::frexp(mx, &e);
+    const double sb = std::ldexp(1.0, 14 - e);
+    (*inv_sb)[fc] = (float)std::ldexp(1.0, e - 14);
+    for (int dir = 0; dir < 26; dir++) {
+      const int dd = dir < 13 ? dir : dir + 1;
+      const int dv[3] = {dd / 9 - 1, (dd / 3) % 3 - 1, dd % 3 - 1};
+      for (int i = 0; i < 8; i++)      // target child
+        for (int j = 0; j < 8; j++) {  // source child
+          const int o[3] = {2 * dv[0] + ((j >> 2) & 1) - ((i >> 2) & 1), 2 * dv[1] + ((j >> 1) & 1) - ((i >> 1) & 1),
+                            2 * dv[2] + (j & 1) - (i & 1)};
+          if (std::max(std::abs(o[0]), std::max(std::abs(o[1]), std::abs(o[2]))) <= 1) continue;  // adjacent
+          const int oi = (o[0] + 3) * 49 + (o[1] + 3) * 7 + (o[2] + 3);
+          for (int fl = 0; fl < H16_F; fl++) {
+            const std::complex<double> t = m2l[(size_t)oi * nf + fc * H16_F + fl] * sb;
+            // rows 2i + (re, im), columns 2j + (re, im): [[re, -im], [im, re]]
+            const double b[2][2] = {{t.real(), -t.imag()}, {t.imag(), t.real()}};
+            unsigned short* blk = img->data() + ((size_t)fc * 26 + dir) * (H16_IMG_BYTES / 2) + fl * 512;
+            for (int a = 0; a < 2; a++)
+              for (int cc = 0; cc < 2; cc++) {
+                // K order of the A rows: column 2 c + e of a block = child c + 4 e
+                const int n = 2 * i + a, k = 2 * (2 * (j & 3) + (j >> 2)) + cc;
+                const __half hi = __float2half_rn((float)b[a][cc]);
+                const __half lo = __float2half_rn((float)(b[a][cc] - (double)__half2float(hi)));
+                // (row, k): K-adjacent core matrices 512 B apart, row groups
+                // of 8 128 B apart, rows 16 B apart; rows 16-31 hold the tails
+                auto at = [&](int row) { return (k / 8) * 256 + (row / 8) * 64 + (row % 8) * 8 + (k % 8); };
+                blk[at(n)] = __half_as_ushort(hi);
+                blk[at(16 + n)] = __half_as_ushort(lo);
+              }
+          }
+        }
+    }
+  }
+}
+
+void launch_spectra_bound(const float* supeden, const int* nodes, int n, const int* depth, int rootlvl, int deg,
+                          int nsurf, unsigned* bound, int num_sms, cudaStream_t st) {
+  cudaMemsetAsync(bound, 0, sizeof(unsigned), st);
+  if (n <= 0) return;
+  const int grid = std::max(1, std::min(num_sms * 4, (n + 7) / 8));
+  k_spectra_bound<<<grid, 256, 0, st>>>(supeden, nodes, n, depth, rootlvl, deg, nsurf, bound);
+}
+
+void launch_m2l_hadamard_tc16(int groups, int nf, const unsigned short* img, const unsigned* spectra, int nq,
+                              const int* qchd, const int* ctab, const unsigned* tile_dirs, float* effval,
+                              const unsigned* bound, const float* inv_sb, int wait_limit, int* status, int num_sms,
+                              cudaStream_t st) {
+  const unsigned char* im = reinterpret_cast<const unsigned char*>(img);
+  if (nf == 868)
+    had_tc16_launch<868>(groups, im, spectra, nq, qchd, ctab, tile_dirs, effval, bound, inv_sb, wait_limit, status,
+                         num_sms, st);
+  else if (nf == 260)
+    had_tc16_launch<260>(groups, im, spectra, nq, qchd, ctab, tile_dirs, effval, bound, inv_sb, wait_limit, status,
+                         num_sms, st);
+  else if (nf == 2052)
+    had_tc16_launch<2052>(groups, im, spectra, nq, qchd, ctab, tile_dirs, effval, bound, inv_sb, wait_limit, status,
+                          num_sms, st);
+}
+
+void m2l_tc16_tables(int nq, int zero_node, const int* coll, std::vector<int>* ctab) {
+  const int ntiles = (nq + H16_M - 1) / H16_M;
+  ctab->assign((size_t)ntiles * 26 * H16_M, (zero_node + 7) >> 3);
+  for (int q = 0; q < nq; q++)
+    for (int d = 0; d < 26; d++)
+      (*ctab)[((size_t)(q / H16_M) * 26 + d) * H16_M + q % H16_M] = (coll[(size_t)q * 26 + d] + 7) >> 3;
+}
+
+}  // namespace kifmm

@@ -413,7 +413,7 @@ __global__ void __launch_bounds__(32 * NWARP) k_leaf_warp(P2PArgs<T> a, const in
     const double cx = a.center[3 * g], cy = a.center[3 * g + 1], cz = a.center[3 * g + 2];
     const T rad = (T)a.radius[g];
     const int tb0 = a.tbeg[g], nt = a.tcnt[g];
-    const bool l2t = a.depth[g] >= 2;
+    const bool l2t = a.depth[g] >= a.l2t_depth;
     const int64_t nb = nptr[wi], ne = nptr[wi + 1];
     const int64_t mb = mptr[wi], me = mptr[wi + 1];
     const int nsurf_segs = (int)(me - mb) + (l2t ? 1 : 0);
@@ -677,6 +677,19 @@ __global__ void k_gather_val(const T* tval, const int* perm, int nt, int td, int
   }
 }
 
+// trgval[r][perm[i]][t] = tval[r][i][t] + near[r][i][t]: the FP32 passes'
+// potentials plus an FP64 near-field sum
+__global__ void k_gather_val_sum(const float* tval, const double* near, const int* perm, int nt, int td, int nrhs,
+                                 double* trgval) {
+  size_t n = (size_t)nt * td * nrhs;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    size_t r = e / ((size_t)nt * td);
+    size_t rem = e % ((size_t)nt * td);
+    int i = (int)(rem / td), d = (int)(rem % td);
+    trgval[r * nt * td + (size_t)perm[i] * td + d] = (double)tval[e] + near[e];
+  }
+}
+
 template <typename T, int KT>
 void launch_p2p_kt(const P2PArgs<T>& a, const P2PWork& w, int which, int rhs, cudaStream_t st) {
   switch (which) {
@@ -757,6 +770,14 @@ void launch_gather_val(const T* tval, const int* perm, int nt, int td, int nrhs,
   k_gather_val<T><<<grid, 256, 0, st>>>(tval, perm, nt, td, nrhs, trgval);
 }
 template void launch_gather_val<double>(const double*, const int*, int, int, int, double*, cudaStream_t);
+
+void launch_gather_val_sum(const float* tval, const double* near, const int* perm, int nt, int td, int nrhs,
+                           double* trgval, cudaStream_t st) {
+  size_t n = (size_t)nt * td * nrhs;
+  if (!n) return;
+  int grid = (int)std::min<size_t>((n + 255) / 256, 148 * 16);
+  k_gather_val_sum<<<grid, 256, 0, st>>>(tval, near, perm, nt, td, nrhs, trgval);
+}
 template void launch_gather_val<float>(const float*, const int*, int, int, int, double*, cudaStream_t);
 
 }  // namespace kifmm

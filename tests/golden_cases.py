@@ -1,4 +1,12 @@
-"""Loader for the committed golden fixtures (made by tests/golden/make_golden.py)."""
+"""Loaders for the committed golden fixtures.
+
+* ``<name>.npz``      small cases with full inputs, outputs, tree and lists
+                      (made by tests/golden/make_golden.py);
+* ``cfg_<name>.npz``  the benchmark configurations at full size: reference
+                      output and direct sum at the check targets only; the
+                      inputs are regenerated from their seeds by workloads.py
+                      (made by tests/golden/make_config_golden.py).
+"""
 import glob
 import os
 
@@ -8,7 +16,8 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 
 def names():
-    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz")))
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz"))
+                  if not os.path.basename(p).startswith("cfg_"))
 
 
 def load(name):
@@ -26,3 +35,18 @@ def options(d, precision=None):
     if precision:
         o["-fmm3d_precision"] = precision
     return o
+
+
+def config_names():
+    return sorted(os.path.basename(p)[4:-4] for p in glob.glob(os.path.join(GOLDEN, "cfg_*.npz")))
+
+
+def load_config(name):
+    z = np.load(os.path.join(GOLDEN, "cfg_" + name + ".npz"))
+    d = {k: z[k] for k in z.files}
+    for k in ("kt", "np_", "ptsmax", "maxlevel", "n"):
+        d[k] = int(d[k])
+    d["workload"] = str(d["workload"])
+    for k in ("ref_relerr", "ref_setup_s", "ref_first_eval_s", "ref_direct_s"):
+        d[k] = float(d[k])
+    return d

@@ -242,18 +242,19 @@ def test_toeplitz_hadamard_matches_direct_form(gpu, name, precision, tol):
     assert diff <= tol, diff
 
 
+@pytest.mark.parametrize("tensor_form", ["tensor", "tensor_tf32"])
 @pytest.mark.parametrize("name", ["lap_s_np6_tt_style", "lap_s_np4_sphere", "lap_s_np8_plummer", "stk_s_np6_cube"])
-def test_tensor_core_hadamard_matches_toeplitz_form(gpu, name):
-    """The V-list product on the tensor cores (split-TF32 MMAs with the
-    gathered colleague spectra in TMEM) against the FP32 Toeplitz-factored
-    product: the same sums to split-TF32 accuracy (5e-6 relative), and both
-    as accurate against the reference as the mixed engine must be.  Stokes
-    (three dofs) has no tensor-core form and keeps the factored one, bit for
-    bit."""
+def test_tensor_core_hadamard_matches_toeplitz_form(gpu, name, tensor_form):
+    """The V-list product on the tensor cores (FP16-pair MMAs, the default,
+    or split-TF32 MMAs, with the gathered colleague spectra in TMEM) against
+    the FP32 Toeplitz-factored product: the same sums to split accuracy
+    (5e-6 relative), and both as accurate against the reference as the
+    mixed engine must be.  Stokes (three dofs) has no tensor-core form and
+    keeps the factored one, bit for bit."""
     d = G.load(name)
     td = W.KERNEL_DOFS[d["kt"]][1]
     outs = []
-    for form in ("tensor", "toeplitz"):
+    for form in (tensor_form, "toeplitz"):
         f = kifmm.FMM3d("fmm3d_")
         f.srcpos, f.srcnor, f.trgpos = d["src"], d["nor"], d["trg"]
         f.ctr, f.rootlvl = tuple(d["ctr"]), d["rootlvl"]
