@@ -8,33 +8,43 @@ seeded synthetic data (no dataset is involved).  A step is one FMM3d::eval
 point cloud; setup (tree, lists, operators) is done once, outside timing.
 
   value      Mpoints/s of the mixed-precision engine (FP32 point sums and
-             spectra, V-list Hadamard and surface contractions in split TF32
-             on the tensor cores), all ranks together
+             spectra, V-list Hadamard on the tensor cores with FP16-pair
+             operands, surface contractions in split TF32), all ranks
   fp64       the plain FP64 GPU engine on the same workload
   batched    64 independent instances (48 Laplace + 16 Stokes single-layer,
              np=6, log-uniform sizes in [1e4, 5e5], sphere / cube / Plummer
-             ball), 8 density vectors each, as one captured CUDA graph:
-             aggregate point-evaluations/s, mixed and FP64, with per-instance
-             errors against the direct sum
+             ball), 8 density vectors each, as one captured CUDA graph;
+             under torchrun every rank evaluates its longest-processing-time
+             share of the instances; aggregate point-evaluations/s, mixed and
+             FP64, per-instance errors against the direct sum
+  configs    the three plain FP64 benchmark configurations at full size
+             (32,768-point sphere, Laplace np=4; 262,144-point ellipsoid,
+             Stokes double layer np=6; 1,048,576-point sphere, Navier np=8)
+             and the cube + Plummer cloud at 262,144 points: Mpoints/s and
+             error against the reference's own direct sum and error at the
+             same check targets (committed fixtures made from the reference)
   e2e        Mpoints/s through the host-pointer C API (kifmm_eval): H2D of the
              densities and D2H of the potentials inside the timed region
   relerr     ||fmm - direct|| / ||fmm|| at 4096 check targets against the
              FP64 direct sum (the reference's FMM3d::check metric)
   cpu_baseline  the reference's own CPU eval (oracle/_ref, built from the
-             reference sources) on a 65,536-point sample of the same cloud,
-             one host thread, rank 0 at N=1 only
-  roofline   the dominant kernel, k_m2l_had_tc (V-list Hadamard): algorithmic
-             flops (8 per V-list pair and stored frequency) over its CUDA-event
-             time against the TF32 dense rate (half the measured bf16 rate),
-             with the executed tensor rate, the algorithmic HBM rate and the
-             DRAM traffic scaled from an ncu capture beside it
+             reference sources) on the workload's cloud at 262,144 points and
+             on the 32,768-point sphere, one host thread, rank 0 at N=1 only
+  roofline   the dominant kernel, k_m2l_had_tc16 (V-list Hadamard): its
+             binding roof is HBM (algorithmic bytes = every source spectrum
+             read once + every accumulated spectrum written once + the
+             operator images), with the tensor rate beside it; plus the
+             whole-eval sum over phases of each phase's bound time over the
+             eval time
 
 --impl reference runs the reference's CPU eval instead, one process per host
-core on independent 65,536-point samples, and reports their aggregate.
+core on independent 262,144-point samples of the workload's cloud, and
+reports their aggregate.
 
-Multi-GPU (torchrun): every rank evaluates its own replica of the workload
-(the single-instance FMM does not shard), so scaling is weak and the value is
-the total points of all ranks over the slowest rank's time.
+Multi-GPU (torchrun): every rank evaluates its own replica of the headline
+workload (one FMM instance does not shard), so scaling is weak and the value
+is the total points of all ranks over the slowest rank's time; the batched
+instances are sharded across ranks.
 """
 from __future__ import annotations
 
@@ -56,11 +66,13 @@ sys.path.insert(0, PKG)
 import workloads as W  # noqa: E402
 
 N_POINTS = 4194304
-SAMPLE = 65536
+SAMPLE = 262144          # the reference arm's and the CPU baseline's sample of the workload's cloud
+SAMPLE_SMALL = 32768     # the 32,768-point sphere (Laplace np=4), the reference's full configuration
 NCHK = 4096
 OPTS = {"-fmm3d_np": "6", "-fmm3d_let3d_ptsmax": "64", "-fmm3d_let3d_maxlevel": "10"}
 METRIC = "Mpoints/s per FMM eval at rel err <=1e-5: batched FP32 vs plain FP64 GPU"
 WORKLOAD = "laplace_cube_plummer_np6"
+GOLDEN = os.path.join(ROOT, "tests", "golden")
 
 
 def parse():
@@ -73,6 +85,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-configs", action="store_true")
     return ap.parse_args()
 
 
@@ -80,22 +93,40 @@ def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
 
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return "unknown"
+
+
 # ---------------------------------------------------------------------------
 # reference arm / CPU baseline
 # ---------------------------------------------------------------------------
-def _ref_worker(n, steps, warmup, seed):
+def _ref_worker(which, n, steps, warmup, seed):
     """One reference instance: setup + warmup + timed evals.  Prints JSON."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
-    p, _ = W.cube_plummer(n, seed)
-    den = W.densities(n, 1, "uniform", 1 + seed)
-    val, times = oracle.ref_fmm(111, [1.0], 6, 64, 10, np.zeros(3), 0, p, p, p, den, neval=warmup + steps)
+    if which == "sphere":
+        wl = W.WORKLOADS["laplace_sphere_np4"]
+        p, nor = W.sphere(n, seed)
+        den = W.densities(n, 1, "uniform", 1 + seed)
+        val, times = oracle.ref_fmm(111, [1.0], wl.np_, wl.ptsmax, wl.maxlevel, np.zeros(3), 0, p, nor, p, den,
+                                    neval=warmup + steps)
+    else:
+        p, _ = W.cube_plummer(n, seed)
+        den = W.densities(n, 1, "uniform", 1 + seed)
+        val, times = oracle.ref_fmm(111, [1.0], 6, 64, 10, np.zeros(3), 0, p, p, p, den, neval=warmup + steps)
     print(json.dumps({"setup_s": times[0], "evals_s": list(times[1 + warmup:])}))
 
 
-def run_reference_procs(nproc, n, steps, warmup):
+def run_reference_procs(nproc, which, n, steps, warmup):
     env = dict(os.environ, OPENBLAS_NUM_THREADS="1", OMP_NUM_THREADS="1")
-    procs = [subprocess.Popen([sys.executable, os.path.abspath(__file__), "--_ref-worker", str(n), str(steps),
+    procs = [subprocess.Popen([sys.executable, os.path.abspath(__file__), "--_ref-worker", which, str(n), str(steps),
                                str(warmup), str(i)], stdout=subprocess.PIPE, stderr=subprocess.PIPE, env=env, text=True)
              for i in range(nproc)]
     outs = []
@@ -129,7 +160,7 @@ def reference_arm(args):
         print(json.dumps({"impl": "reference", "unavailable": "reference library oracle/_ref/libkifmm_ref.so not built"}))
         return
     nproc = max(1, min(host_cores(), 64))
-    outs = run_reference_procs(nproc, SAMPLE, args.steps, args.warmup)
+    outs = run_reference_procs(nproc, "cube_plummer", SAMPLE, args.steps, args.warmup)
     # step k = the k-th eval of every process, running concurrently
     step_s = [max(o["evals_s"][k] for o in outs) for k in range(args.steps)]
     ms = 1e3 * statistics.mean(step_s)
@@ -140,8 +171,10 @@ def reference_arm(args):
             "config": {"workload": WORKLOAD, "n_points_per_instance": SAMPLE, "instances": nproc, "kernel": 111,
                        "np": 6, "ptsmax": 64, "maxlevel": 10, "precision": "fp64 (reference CPU)"},
             "cpu_baseline": {"value": value, "unit": "Mpoints/s", "cores": nproc, "kind": "reference",
-                             "sample": f"{nproc} independent {SAMPLE}-point instances of the workload's cloud, "
-                                       f"one reference process per core, OPENBLAS_NUM_THREADS=1"},
+                             "cpu": cpu_model(),
+                             "sample": f"{nproc} independent {SAMPLE}-point instances of the workload's cloud "
+                                       f"(70% cube + 30% Plummer), one reference process per core, "
+                                       f"OPENBLAS_NUM_THREADS=1"},
             "e2e": {"value": value, "unit": "Mpoints/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -198,25 +231,70 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
-# engine arm
+# peaks and roofline model
 # ---------------------------------------------------------------------------
-def peaks():
-    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
-    try:
-        with open(path) as f:
-            d = json.load(f)
-        return d["hbm_gbs"], "measured"
-    except Exception:
-        return 6650.0, "fallback"
-
-
-def peak_bf16():
-    """Measured dense bf16 TFLOP/s (burst) of this pool's B200s, else None."""
+def measured_peaks():
+    """(HBM GB/s, bf16 TFLOP/s burst, SM max MHz, kind) from MEASURED_PEAKS.json, else the fallback."""
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
-            return float(json.load(f)["bf16_tflops"])
+            d = json.load(f)
+        return float(d["hbm_gbs"]), float(d["bf16_tflops"]), float(d.get("sm_max_mhz", 1965.0)), "measured"
     except Exception:
-        return None
+        return 6650.0, 1590.0, 1965.0, "fallback"
+
+
+NF6 = 4 * 6 ** 3 + 4  # stored (Hermitian-canonical) frequencies per spectrum at np=6
+NSURF6 = 6 ** 3 - 4 ** 3  # |UE| = |DC| at np=6
+# DRAM bytes (read + write) of one k_m2l_had_tc16 launch per spectrum node,
+# from an ncu capture of that kernel (dram__bytes_read.sum +
+# dram__bytes_write.sum) on the 1,048,576-point cloud of this workload,
+# scaled by the number of spectra of the workload timed here
+HAD_TRAFFIC_PER_SPECTRUM = 13680.0
+
+
+def roofline(phases, wc, hbm, bf16, sm_mhz, had_ms):
+    """The dominant kernel's roofline (HBM-bound Hadamard) and the whole-eval
+    sum over phases of each phase's bound time over the eval time."""
+    gbs = hbm * 1e9
+    tensor16 = bf16 * 1e12          # FP16/BF16 dense rate (the Hadamard's MMAs)
+    tf32 = tensor16 / 2             # TF32 dense rate (the surface contractions)
+    mufu = 148 * 16 * sm_mhz * 1e6  # FP32 reciprocal square roots per second (16 per SM per clock)
+    spec_b = NF6 * 8                # one spectrum: complex FP32 (or its FP16 pair) per stored frequency
+    img_b = (NF6 // 4) * 26 * 4096  # FP16 operator images, one per (chunk of 4 frequencies, direction)
+    had_bytes = (wc["fwd_spectra"] + wc["inv_spectra"]) * spec_b + img_b
+    had_flops = wc["v_pairs"] * NF6 * 8
+    had = {"bound": "hbm", "kernel": "k_m2l_had_tc16 (V-list Hadamard on tcgen05, FP16-pair operands)",
+           "achieved": had_bytes / (had_ms / 1e3) / 1e9, "peak": hbm, "unit": "GB/s",
+           "frac": had_bytes / (had_ms / 1e3) / gbs, "traffic": HAD_TRAFFIC_PER_SPECTRUM * wc["fwd_spectra"],
+           "traffic_unit": "bytes per launch", "algorithmic_bytes": had_bytes, "kernel_ms": had_ms,
+           "tensor_achieved_tflops": had_flops / (had_ms / 1e3) / 1e12, "tensor_peak_tflops": bf16,
+           "tensor_frac": had_flops / (had_ms / 1e3) / tensor16,
+           "t_bound_ms": 1e3 * max(had_bytes / gbs, had_flops / tensor16)}
+    # whole eval: per phase the time its binding roof allows
+    fwd_bytes = wc["fwd_spectra"] * (spec_b + NSURF6 * 4)
+    inv_bytes = wc["inv_spectra"] * (spec_b + NSURF6 * 4)
+    bound = {
+        "m2l_forward": fwd_bytes / gbs,
+        "m2l_hadamard": had["t_bound_ms"] / 1e3,
+        "m2l_inverse": inv_bytes / gbs,
+        "surface_contractions": wc["gemm_flops"] / tf32,
+        "point_sums": (wc["near_interactions"] + wc["surface_interactions"]) / mufu,
+    }
+    measured = {"m2l_forward": phases["m2l_forward"], "m2l_hadamard": phases["m2l_hadamard"],
+                "m2l_inverse": phases["m2l_inverse"],
+                "surface_contractions": phases["upward"] + phases["downward"],
+                "point_sums": phases["leaf"] + phases["xlist"]}
+    total_bound = sum(bound.values())
+    whole = {"achieved_ms": phases["total"], "bound_ms": 1e3 * total_bound, "frac": 1e3 * total_bound / phases["total"],
+             "phases": {k: {"bound_ms": 1e3 * bound[k], "measured_ms": measured[k],
+                            "frac": 1e3 * bound[k] / measured[k] if measured[k] > 0 else None} for k in bound},
+             "roofs": {"m2l_forward": "HBM: node densities read + spectra written",
+                       "m2l_hadamard": "HBM: spectra read once + accumulated spectra written once + images",
+                       "m2l_inverse": "HBM: accumulated spectra read + check values written",
+                       "surface_contractions": "TF32 tensor rate (half the measured bf16 rate), flops counted once",
+                       "point_sums": "reciprocal square roots, 16 per SM per clock at the maximum SM clock "
+                                     "(one per interaction; Laplace)"}}
+    return had, whole
 
 
 BATCH_RHS = 8
@@ -224,69 +302,130 @@ BATCH_NCHK = 256
 
 
 def batched_section(torch, kifmm, stream, flush, steps, warmup, precision, pg=None):
-    """64 independent instances (48 Laplace + 16 Stokes single-layer, np=6,
-    log-uniform sizes in [1e4, 5e5], sphere / cube / Plummer ball), 8 density
-    vectors each, evaluated as one captured CUDA graph (kifmm_batch_eval_device).
-    Returns the aggregate point-evaluations per second and per-instance errors
-    against the FP64 direct sum (first and last density vector, 256 targets)."""
-    insts = W.batched_instances()
-    fmms, srcs, outs, dens, pts = [], [], [], [], []
-    t0 = time.perf_counter()
-    for inst in insts:
-        p, _ = W.GEOMETRIES[inst["geometry"]](inst["n"], inst["seed"])
-        f = kifmm.FMM3d("fmm3d_")
-        f.srcpos = f.srcnor = f.trgpos = p
-        f.knl = kifmm.Kernel3d(inst["kt"], list(inst["coefs"]))
-        o = dict(OPTS)
-        o["-fmm3d_precision"] = precision
-        f.setup(o)
-        sd, td = W.KERNEL_DOFS[inst["kt"]]
-        den = W.densities(inst["n"] * BATCH_RHS, sd, "uniform", inst["seed"] + 1)
-        fmms.append(f)
-        dens.append(den)
-        pts.append(p)
-        srcs.append(torch.tensor(den, device="cuda", dtype=torch.float64))
-        outs.append(torch.zeros(inst["n"] * td * BATCH_RHS, device="cuda", dtype=torch.float64))
-    setup_s = time.perf_counter() - t0
-    b = kifmm.Batch(fmms)
-    sp, op = [s.data_ptr() for s in srcs], [o.data_ptr() for o in outs]
-    for _ in range(warmup):
-        b.eval(sp, op, BATCH_RHS, stream.cuda_stream, sync=True)
-    torch.cuda.synchronize()
-    times = []
-    for _ in range(steps):
-        with torch.cuda.stream(stream):
-            flush.fill_(1.0)
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-        b.eval(sp, op, BATCH_RHS, stream.cuda_stream, sync=False)
-        with torch.cuda.stream(stream):
-            e1.record(stream)
-        e1.synchronize()
-        times.append(e0.elapsed_time(e1))
-    ms = statistics.mean(times)
-    if pg is not None:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
-    launches = int(sum(f.last_launch_count() for f in fmms))
+    """The batched workload (workloads.batched_instances), 8 density vectors
+    each, evaluated as one captured CUDA graph (kifmm_batch_eval_device).
+    Every rank sets up and evaluates only its longest-processing-time share
+    of the instances (multigpu.batched_run); the value is all instances'
+    point-evaluations over the slowest rank's time."""
+    import multigpu
+    rank = pg.get_rank() if pg is not None else 0
     world = pg.get_world_size() if pg is not None else 1
-    errs = []
-    for inst, f, den, p, out in zip(insts, fmms, dens, pts, outs):
-        n = inst["n"]
-        sd, td = W.KERNEL_DOFS[inst["kt"]]
-        chk = W.check_indices(n, BATCH_NCHK, inst["seed"] + 2)
-        val = out.cpu().numpy().reshape(BATCH_RHS, n, td)
-        for r in (0, BATCH_RHS - 1):
-            direct = f.direct(den[r * n * sd:(r + 1) * n * sd], p[chk]).reshape(-1, td)
-            got = val[r][chk]
-            errs.append(float(np.linalg.norm(direct - got) / np.linalg.norm(got)))
-    npts = sum(i["n"] for i in insts)
-    del b
-    return {"value": world * npts * BATCH_RHS / (ms / 1e3) / 1e6, "unit": "Mpoints/s", "ms_per_step": ms,
-            "relerr_max": max(errs), "relerr_median": statistics.median(errs), "setup_s": setup_s,
-            "launches_per_step": launches, "points_per_instance_total": npts}
+    insts_all = W.batched_instances()
+
+    def run_shard(mine):
+        insts = [insts_all[i] for i in mine]
+        fmms, srcs, outs, dens, pts = [], [], [], [], []
+        t0 = time.perf_counter()
+        for inst in insts:
+            p, _ = W.GEOMETRIES[inst["geometry"]](inst["n"], inst["seed"])
+            f = kifmm.FMM3d("fmm3d_")
+            f.srcpos = f.srcnor = f.trgpos = p
+            f.knl = kifmm.Kernel3d(inst["kt"], list(inst["coefs"]))
+            o = dict(OPTS)
+            o["-fmm3d_precision"] = precision
+            f.setup(o)
+            sd, td = W.KERNEL_DOFS[inst["kt"]]
+            den = W.densities(inst["n"] * BATCH_RHS, sd, "uniform", inst["seed"] + 1)
+            fmms.append(f)
+            dens.append(den)
+            pts.append(p)
+            srcs.append(torch.tensor(den, device="cuda", dtype=torch.float64))
+            outs.append(torch.zeros(inst["n"] * td * BATCH_RHS, device="cuda", dtype=torch.float64))
+        setup_s = time.perf_counter() - t0
+        b = kifmm.Batch(fmms) if fmms else None
+        sp, op = [x.data_ptr() for x in srcs], [x.data_ptr() for x in outs]
+        for _ in range(warmup):
+            if b is not None:
+                b.eval(sp, op, BATCH_RHS, stream.cuda_stream, sync=True)
+        torch.cuda.synchronize()
+        if pg is not None:
+            pg.barrier()
+        times = []
+        for _ in range(steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+            if b is not None:
+                b.eval(sp, op, BATCH_RHS, stream.cuda_stream, sync=False)
+            with torch.cuda.stream(stream):
+                e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        if b is not None:
+            b.poll_status()  # a device-side wait that timed out in a timed replay raises here
+        launches = int(sum(f.last_launch_count() for f in fmms))
+        errs = []
+        for inst, f, den, p, out in zip(insts, fmms, dens, pts, outs):
+            n = inst["n"]
+            sd, td = W.KERNEL_DOFS[inst["kt"]]
+            chk = W.check_indices(n, BATCH_NCHK, inst["seed"] + 2)
+            val = out.cpu().numpy().reshape(BATCH_RHS, n, td)
+            for r in (0, BATCH_RHS - 1):
+                direct = f.direct(den[r * n * sd:(r + 1) * n * sd], p[chk]).reshape(-1, td)
+                got = val[r][chk]
+                # FMM3d::check's metric (fmm3d/fmm3d_check.cpp:61-69): ||fmm - direct|| / ||fmm||
+                errs.append((float(np.linalg.norm(direct - got) / np.linalg.norm(got)), inst["index"], r))
+        del b
+        return statistics.mean(times), {"errs": errs, "setup_s": setup_s, "launches": launches}
+
+    res = multigpu.batched_run(insts_all, rank, world, run_shard, rhs=BATCH_RHS, dist=pg,
+                               device=torch.device("cuda"))
+    extra = res["extra"]
+    errs = extra["errs"]
+    worst = max(errs) if errs else (0.0, -1, 0)
+    rel = [e[0] for e in errs]
+    return {"value": res["value"], "unit": "Mpoints/s", "ms_per_step": res["ms"],
+            "relerr_max": worst[0], "relerr_max_instance": worst[1],
+            "relerr_median": statistics.median(rel) if rel else None,
+            "instances_over_1e-5": sorted({e[1] for e in errs if e[0] > 1e-5}),
+            "setup_s": extra["setup_s"], "launches_per_step": extra["launches"],
+            "points_per_instance_total": sum(i["n"] for i in insts_all), "instances_this_rank": len(res["mine"]),
+            "lpt_imbalance": res["imbalance"]}
+
+
+def config_section(kifmm, stream_handle, steps):
+    """The benchmark configurations at full size against the reference's own
+    results at the same check targets (fixtures made by
+    tests/golden/make_config_golden.py from the reference itself)."""
+    out = {}
+    for name in ("laplace_sphere_np4", "stokes_dl_ellipsoid_np6", "navier_sphere_np8", "laplace_cube_plummer_np6_262k"):
+        path = os.path.join(GOLDEN, "cfg_" + name + ".npz")
+        if not os.path.exists(path):
+            continue
+        z = np.load(path)
+        wl = W.WORKLOADS[str(z["workload"])]
+        n = int(z["n"])
+        p, nor = wl.points(n)
+        den = wl.density(n)
+        td = wl.tdof
+        rec = {"n_points": n, "kernel": wl.kt, "np": wl.np_, "ptsmax": wl.ptsmax, "ref_relerr": float(z["ref_relerr"]),
+               "ref_cpu_first_eval_s": float(z["ref_first_eval_s"])}
+        for prec in ("fp64", "mixed"):
+            f = kifmm.FMM3d("fmm3d_")
+            f.srcpos, f.srcnor, f.trgpos = p, nor, p
+            f.knl = kifmm.Kernel3d(wl.kt, list(wl.coefs))
+            t0 = time.perf_counter()
+            f.setup({"-fmm3d_np": str(wl.np_), "-fmm3d_let3d_ptsmax": str(wl.ptsmax),
+                     "-fmm3d_let3d_maxlevel": str(wl.maxlevel), "-fmm3d_precision": prec})
+            setup_s = time.perf_counter() - t0
+            vals = np.zeros(td * n)
+            f.eval(den, vals)  # warm-up through the host API
+            f.set_profiling(True)
+            ts = []
+            for _ in range(steps):
+                f.eval(den, vals)
+                ts.append(f.phase_times()["total"])
+            f.set_profiling(False)
+            got = vals.reshape(-1, td)[z["chk"]]
+            err = float(np.linalg.norm(z["ref_direct"] - got) / np.linalg.norm(got))
+            ms = statistics.mean(ts)
+            rec[prec] = {"ms_per_eval": ms, "value": n / (ms / 1e3) / 1e6, "unit": "Mpoints/s", "relerr": err,
+                         "within_10x_reference": bool(err <= 10 * float(z["ref_relerr"])), "setup_s": setup_s}
+            del f
+        out[name] = rec
+    return out
 
 
 def engine_arm(args):
@@ -323,7 +462,7 @@ def engine_arm(args):
         if pg is not None:
             pg.barrier()
 
-    def timed(f, steps, warmup, profile=False):
+    def timed(f, steps, warmup):
         for _ in range(warmup):
             f.eval_device(d_den.data_ptr(), d_out.data_ptr(), 1, stream.cuda_stream, sync=True)
         torch.cuda.synchronize()
@@ -342,6 +481,7 @@ def engine_arm(args):
             e1.synchronize()
             times.append(e0.elapsed_time(e1))
         torch.cuda.synchronize()
+        f.poll_status()  # a device-side wait that timed out in the timed evals raises here
         barrier()
         ms = statistics.mean(times)
         if pg is not None:
@@ -358,10 +498,13 @@ def engine_arm(args):
     clk = clocks.stop()
     launches = fm.last_launch_count()
     out_mixed = d_out.cpu().numpy()
-    # per-kernel device times of one profiled eval (roofline of the dominant kernel)
+    # per-kernel device times of profiled evals (roofline of the dominant kernel)
     fm.set_profiling(True)
-    fm.eval_device(d_den.data_ptr(), d_out.data_ptr(), 1, stream.cuda_stream, sync=True)
-    phases = fm.phase_times()
+    ph_runs = []
+    for _ in range(3):
+        fm.eval_device(d_den.data_ptr(), d_out.data_ptr(), 1, stream.cuda_stream, sync=True)
+        ph_runs.append(fm.phase_times())
+    phases = {k: statistics.median(r[k] for r in ph_runs) for k in ph_runs[0]}
     fm.set_profiling(False)
     wc = fm.work_counters()
     # accuracy (FMM3d::check metric) against the FP64 direct sum on the device
@@ -394,7 +537,8 @@ def engine_arm(args):
         out64 = d_out.cpu().numpy()
         err64 = float(np.linalg.norm(direct - out64[chk]) / np.linalg.norm(out64[chk]))
         fp64 = {"value": world * n / (ms64 / 1e3) / 1e6, "unit": "Mpoints/s", "ms_per_step": ms64,
-                "relerr": err64, "setup_s": setup_fp64, "dtype": "f64"}
+                "relerr": err64, "setup_s": setup_fp64, "dtype": "f64",
+                "mixed_over_fp64": ms64 / ms_mixed}
         del f64
     # ---- batched form: 64 instances x 8 density vectors in one graph
     batched = None
@@ -404,56 +548,56 @@ def engine_arm(args):
                    "kernels": "48 x Laplace SL (111), 16 x Stokes SL (311)",
                    "sizes": "log-uniform in [1e4, 5e5] points", "geometries": "sphere / cube / Plummer ball",
                    "check": f"{BATCH_NCHK} targets per instance, density vectors 0 and {BATCH_RHS - 1}",
+                   "sharding": f"longest-processing-time over {world} rank(s)",
                    "mixed": batched_section(torch, kifmm, stream, flush, bsteps, bwarm, "mixed", pg)}
         if not args.no_fp64:
             batched["fp64"] = batched_section(torch, kifmm, stream, flush, bsteps, bwarm, "fp64", pg)
-    # ---- CPU baseline: the reference on a bounded sample, rank 0, N=1
+            batched["mixed_over_fp64"] = batched["mixed"]["value"] / batched["fp64"]["value"]
+    # ---- the plain configurations at full size, rank 0
+    configs = None
+    if rank == 0 and not args.no_configs:
+        configs = config_section(kifmm, 0, 3)
+    # ---- CPU baseline: the reference on bounded samples, rank 0, N=1
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import oracle
         if oracle.ref_available():
-            o = run_reference_procs(1, SAMPLE, 2, 1)[0]
+            o = run_reference_procs(1, "cube_plummer", SAMPLE, 2, 1)[0]
             s = statistics.mean(o["evals_s"])
-            cpu = {"value": SAMPLE / s / 1e6, "unit": "Mpoints/s", "cores": 1, "kind": "reference",
-                   "sample": f"one {SAMPLE}-point instance of the workload's cloud, mean of 2 evals after 1 warm-up, "
-                             f"reference built from its sources (FFTW2-interface shim, scipy OpenBLAS)"}
+            o2 = run_reference_procs(1, "sphere", SAMPLE_SMALL, 3, 1)[0]
+            s2 = statistics.mean(o2["evals_s"])
+            cpu = {"value": SAMPLE / s / 1e6, "unit": "Mpoints/s", "cores": 1, "kind": "reference", "cpu": cpu_model(),
+                   "host_cores": host_cores(),
+                   "sample": f"the workload's cloud (70% cube + 30% Plummer, Laplace np=6, ptsmax 64) at {SAMPLE} "
+                             f"points, mean of 2 evals after 1 warm-up, one thread; reference built from its "
+                             f"sources (FFTW2-interface shim, scipy OpenBLAS, OPENBLAS_NUM_THREADS=1)",
+                   "sphere_32768_np4": {"value": SAMPLE_SMALL / s2 / 1e6, "unit": "Mpoints/s", "eval_s": s2}}
         else:
             cpu = {"value": None, "unit": "Mpoints/s", "cores": 1, "kind": "reference",
                    "sample": "reference library not built on this host"}
     if rank != 0:
+        if pg is not None:
+            pg.destroy_process_group()
         return
-    hbm, peak_kind = peaks()
-    bf16 = peak_bf16()
-    # dominant kernel: the V-list Hadamard accumulation on the tensor cores
-    # (k_m2l_had_tc).  Algorithmic work = one complex multiply-add (8 flops) per
-    # V-list pair and stored frequency; algorithmic bytes = source spectra read
-    # once + accumulated target spectra written once + the operator images.
-    # Executed tensor work adds the split-TF32 products (head*head, head*tail,
-    # tail*head) and the adjacent-child zero blocks of every parent pair.
-    nf = 4 * 6 ** 3 + 4  # independent (Hermitian-canonical) frequencies at np=6
-    cplx = 8  # FP32 complex
-    alg_bytes = (wc["fwd_spectra"] + wc["inv_spectra"]) * nf * cplx + 26 * nf * 2048
+    hbm, bf16, sm_max, peak_kind = measured_peaks()
     had_ms = phases.get("m2l_hadamard") or phases["vlist"]
-    had_flops = wc["v_pairs"] * nf * 8
-    had_exec_flops = wc.get("tc_hadamard_flops", 0.0)
-    achieved = had_flops / (had_ms / 1e3) / 1e12
-    tf32_peak = bf16 / 2 if bf16 else 1590.0 / 2  # TF32 dense = half the bf16 rate
-    # DRAM traffic per launch: 14,236 B per spectrum node, read + write, from the
-    # ncu capture of this kernel on the 1M-point case (profiles/hadamard_tc_*),
-    # scaled by the spectra of this workload
-    traffic = 14236.0 * wc["fwd_spectra"]
+    had_roof, whole = roofline(phases, wc, hbm, bf16, sm_max, had_ms)
+    had_roof["peak_kind"] = peak_kind + " (STREAM-style copy)"
+    had_roof["whole_eval"] = whole
     line = {
         "metric": METRIC, "value": world * n / (ms_mixed / 1e3) / 1e6, "unit": "Mpoints/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_mixed, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "n_points": n, "kernel": 111, "np": 6, "ptsmax": 64, "maxlevel": 10,
-                   "precision": "mixed (FP32 point sums and spectra; V-list Hadamard and surface contractions "
-                                "in split TF32 on tcgen05 with FP32 accumulation; FP64 operator SVDs)", "rhs": 1,
+                   "precision": "mixed (FP32 point sums and spectra; V-list Hadamard on tcgen05 with FP16-pair "
+                                "operands and FP32 accumulation; surface contractions in split TF32 on tcgen05; "
+                                "FP64 operator SVDs)", "rhs": 1,
                    "l2": "flushed (256 MB write) before every timed step", "parallelism": f"replicas x{world}"},
         "relerr": relerr, "check_targets": NCHK,
         "fp64": fp64,
         "batched": batched,
+        "configs": configs,
         "e2e": {"value": world * n / (e2e_ms / 1e3) / 1e6, "unit": "Mpoints/s",
                 "h2d_bytes_per_step": int(n * 8), "d2h_bytes_per_step": int(n * 8), "ms_per_step": e2e_ms},
         "gpu_launches": int(launches * args.steps),
@@ -461,17 +605,7 @@ def engine_arm(args):
         "phases_ms": phases,
         "work": wc,
         "setup_s": setup_mixed,
-        "roofline": {"bound": "tensor", "kernel": "k_m2l_had_tc (V-list Hadamard on tcgen05, split TF32)",
-                     "achieved": achieved, "peak": tf32_peak, "unit": "TFLOP/s", "frac": achieved / tf32_peak,
-                     "peak_kind": ("measured" if bf16 else "fallback") + " (TF32 dense = half the bf16 burst)",
-                     "traffic": traffic, "traffic_unit": "bytes per launch", "kernel_ms": had_ms,
-                     "algorithmic": "8 flops per V-list pair and stored frequency",
-                     "executed_tensor_tflops": had_exec_flops / (had_ms / 1e3) / 1e12,
-                     "hbm_achieved_gbs": alg_bytes / (had_ms / 1e3) / 1e9, "hbm_peak_gbs": hbm,
-                     "limiter": "round trip of each producer group's TMEM A stage (gather loads, wait for the "
-                                "stage's previous MMAs, split and store, operator images), one third of it per "
-                                "step with three stages; neither the tensor pipe (~18 % active) nor DRAM (~8 % "
-                                "of peak) is saturated"},
+        "roofline": had_roof,
         "clocks": clk,
         "cpu_baseline": cpu,
     }
@@ -482,7 +616,7 @@ def engine_arm(args):
 
 def main():
     if len(sys.argv) > 1 and sys.argv[1] == "--_ref-worker":
-        _ref_worker(int(sys.argv[2]), int(sys.argv[3]), int(sys.argv[4]), int(sys.argv[5]))
+        _ref_worker(sys.argv[2], int(sys.argv[3]), int(sys.argv[4]), int(sys.argv[5]), int(sys.argv[6]))
         return
     args = parse()
     if args.impl == "reference":

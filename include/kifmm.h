@@ -91,6 +91,19 @@ kifmm_status kifmm_eval_multi(kifmm_handle h, int nrhs, const double* srcden, do
 kifmm_status kifmm_eval_device(kifmm_handle h, int nrhs, const double* d_srcden, double* d_trgval, void* stream,
                                int sync);
 
+/* No counterpart in the reference (its eval is synchronous and asserts).
+ * Every pipeline wait inside this library's kernels is bounded; a wait that
+ * runs out sets a bit of the handle's device status word and the kernel
+ * returns without faulting.  Synchronous calls report it as
+ * KIFMM_ERR_CUDA; for kifmm_eval_device(sync = 0) it is reported by the
+ * handle's next kifmm_eval_device call or by this poll, once the stream
+ * has been synchronised: KIFMM_ERR_CUDA if an eval that has completed since
+ * the last poll timed out (the word is read and cleared).  The option
+ * -<prefix>wait_limit (polls per wait, default 4194304) bounds the pipeline
+ * waits of the tensor-core V-list kernel; 0 makes each of them give up at
+ * once, which exercises this path without a fault. */
+kifmm_status kifmm_poll_status(kifmm_handle h);
+
 /* Batched evaluation of independent instances (no counterpart in the
  * reference, which runs one FMM3d::eval at a time, fmm3d/tt.cpp:97-101).
  * A batch groups already set-up handles (any kernels and sizes); each
@@ -105,6 +118,10 @@ kifmm_status kifmm_batch_destroy(kifmm_batch b);
 kifmm_status kifmm_batch_eval_device(kifmm_batch b, int nrhs, const double* const* d_srcden,
                                      double* const* d_trgval, void* stream, int sync);
 const char* kifmm_batch_last_error(kifmm_batch b);
+/* kifmm_poll_status over the batch's instances (synchronous replays poll
+ * themselves; an asynchronous replay's time-out is reported by the next
+ * kifmm_batch_eval_device or by this call after the stream is synchronised). */
+kifmm_status kifmm_batch_poll_status(kifmm_batch b);
 
 /* Replaces FMM3d::check(srcden, trgval, numchk) (fmm3d/fmm3d_check.cpp:25-73):
  * FP64 direct sum at numchk targets picked with `seed`; returns
@@ -126,9 +143,12 @@ kifmm_status kifmm_direct(kifmm_handle h, const double* srcden, int nt, const do
  * its partial sums live in one fixed device array of
  * KIFMM_NOALLOC_SCRATCH_DOUBLES doubles (8 MiB, held on every GPU that loads
  * the library until exit), so nt * tdof above that limit returns
- * KIFMM_ERR_CAPACITY.  The first call on a device looks the array up
- * (cudaGetSymbolAddress) and should come before any stream capture.  All
- * calls share the array: calls that overlap on the GPU race and must be
+ * KIFMM_ERR_CAPACITY.  Every call looks the array up on the current device
+ * (cudaGetSymbolAddress, which allocates nothing); the first call on a
+ * device loads the module there and should come before any stream capture.
+ * An error already pending from the caller's earlier work is returned as
+ * KIFMM_ERR_CUDA before anything is launched, and left pending.  All calls
+ * share the array: calls that overlap on the GPU race and must be
  * serialised by the caller. */
 #define KIFMM_NOALLOC_SCRATCH_DOUBLES (1 << 20)
 kifmm_status kifmm_direct_noalloc(int kt, int ncoef, const double* coefs, int ns, const double* d_srcpos,

@@ -135,7 +135,19 @@ kifmm_status kifmm_batch_eval_device(kifmm_batch b, int nrhs, const double* cons
     b->err = cudaGetErrorString(cudaGetLastError());
     return KIFMM_ERR_CUDA;
   }
+  if (sync) return kifmm_batch_poll_status(b);
   return KIFMM_OK;
+}
+
+kifmm_status kifmm_batch_poll_status(kifmm_batch b) {
+  if (!b) return KIFMM_ERR_ARG;
+  kifmm_status rc = KIFMM_OK;
+  for (size_t i = 0; i < b->hs.size(); i++)
+    if (b->hs[i]->e.poll_status() != KIFMM_OK) {
+      b->err = "instance " + std::to_string(i) + ": " + b->hs[i]->e.err;
+      rc = KIFMM_ERR_CUDA;
+    }
+  return rc;
 }
 
 const char* kifmm_batch_last_error(kifmm_batch b) { return b ? b->err.c_str() : "null batch"; }

@@ -99,6 +99,11 @@ kifmm_status kifmm_eval_device(kifmm_handle h, int nrhs, const double* d_srcden,
   return (kifmm_status)h->e.eval_device(d_srcden, d_trgval, nrhs, (cudaStream_t)stream, sync != 0);
 }
 
+kifmm_status kifmm_poll_status(kifmm_handle h) {
+  if (!h) return KIFMM_ERR_ARG;
+  return (kifmm_status)h->e.poll_status();
+}
+
 kifmm_status kifmm_check(kifmm_handle h, const double* srcden, const double* trgval, int numchk, uint64_t seed,
                          double* relerr) {
   if (!h || !srcden || !trgval || !relerr) return KIFMM_ERR_ARG;

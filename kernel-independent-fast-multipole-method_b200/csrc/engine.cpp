@@ -908,8 +908,8 @@ int Engine::setup() {
     m2l_tc = mixed && tensor_cores;
     m2l_tc_tf32 = false;
     int wl = 1 << 22;
-    if (!parse_int(opts, "-" + prefix + "wait_limit", &wl, &found) || wl < 1) {
-      err = "wait_limit must be a positive integer";
+    if (!parse_int(opts, "-" + prefix + "wait_limit", &wl, &found) || wl < 0) {
+      err = "wait_limit must be a non-negative integer";
       return KIFMM_ERR_OPTION;
     }
     wait_limit = wl;
@@ -1006,6 +1006,9 @@ int Engine::eval_device(const double* d_srcden, double* d_trgval, int nrhs, cuda
     err = "bad eval arguments";
     return KIFMM_ERR_ARG;
   }
+  // a time-out of an earlier asynchronous eval surfaces at the next call,
+  // the way CUDA reports errors of earlier asynchronous launches
+  if (!sync && poll_status() != KIFMM_OK) return KIFMM_ERR_CUDA;
   try {
     int rc = impl->eval(d_srcden, d_trgval, nrhs, st);  // st as given: NULL is the legacy default stream
     if (rc != KIFMM_OK) return rc;
@@ -1019,6 +1022,19 @@ int Engine::eval_device(const double* d_srcden, double* d_trgval, int nrhs, cuda
   } catch (const CudaError& e) {
     err = std::string(e.where) + ": " + cudaGetErrorString(e.e);
     cudaGetLastError();
+    return KIFMM_ERR_CUDA;
+  }
+  return KIFMM_OK;
+}
+
+int Engine::poll_status() {
+  if (!ready) {
+    err = "poll before a successful setup";
+    return KIFMM_ERR_STATE;
+  }
+  const int v = impl->take_status();
+  if (v) {
+    err = "a device-side wait timed out (status bits " + std::to_string(v) + "); the results of that eval are incomplete";
     return KIFMM_ERR_CUDA;
   }
   return KIFMM_OK;

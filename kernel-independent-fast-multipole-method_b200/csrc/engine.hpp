@@ -43,7 +43,8 @@ struct Engine {
   bool m2l_toeplitz = false;  // V-list Hadamard in the 2x2x2 block-Toeplitz factored form
   bool m2l_tc = false;        // mixed, single-dof kernels: V-list Hadamard on tcgen05
   bool m2l_tc_tf32 = false;   // ... with split-TF32 operands instead of FP16 pairs
-  int wait_limit = 1 << 22;   // polls before a device-side pipeline wait gives up (-<prefix>wait_limit)
+  int wait_limit = 1 << 22;   // polls before a device-side pipeline wait gives up (-<prefix>wait_limit;
+                              // 0: every such wait gives up at once, to exercise the time-out path)
   int had_groups = 3;         // producer groups of the FP16 tensor-core Hadamard (-<prefix>had_groups)
   bool profiling = false;
   // state
@@ -73,6 +74,9 @@ struct Engine {
   // or error query (usable inside a stream capture).
   int enqueue(const double* d_srcden, double* d_trgval, int nrhs, cudaStream_t st);
   int reserve(int nrhs);
+  // KIFMM_ERR_CUDA if a device-side wait of an evaluation that has completed
+  // since the last poll timed out (the status word is read and cleared)
+  int poll_status();
   int direct(const double* srcden, int nt_chk, const double* tpos, double* out);
   int check(const double* srcden, const double* trgval, int numchk, uint64_t seed, double* relerr);
   void release_device();

@@ -23,13 +23,13 @@
 // two calls whose kernels overlap on the GPU (different streams, or
 // different host threads) race on it and must be serialised by the caller.
 //
-// The array's device address is looked up once per device with
-// cudaGetSymbolAddress (host code cannot use the symbol itself: on the host
-// it names a stand-in, not device memory) during the first call on that
-// device, with that device current.  That first call should therefore come
-// before any stream capture.
+// The array's device address is looked up with cudaGetSymbolAddress on
+// every call, with the caller's device current (host code cannot use the
+// symbol itself: on the host it names a stand-in, not device memory); the
+// lookup allocates nothing and stays right after a cudaDeviceReset, which
+// reloads the module and may move the array.  The first call on a device
+// loads the module there and should come before any stream capture.
 #include <algorithm>
-#include <mutex>
 
 #include "../../include/kifmm.h"
 #include "kernels_common.cuh"
@@ -42,10 +42,6 @@ static __device__ __align__(256) double g_noalloc_scratch[KIFMM_NOALLOC_SCRATCH_
 constexpr int NA_THREADS = 128;
 constexpr int NA_TILE = 128;
 constexpr int NA_MAXCHUNK = 64;
-constexpr int NA_MAXDEV = 64;
-
-std::mutex g_mu;
-double* g_scratch_ptr[NA_MAXDEV] = {nullptr};
 
 // partial[c][t][d] = sum over sources of chunk c of K(trg_t - src) den
 template <int KT>
@@ -61,23 +57,23 @@ __global__ void __launch_bounds__(NA_THREADS) k_direct_partial(const double* __r
   const int s1 = min(ns, s0 + chunk);
   double px = 0, py = 0, pz = 0;
   if (t < nt) {
-    px = tpos[3 * t];
-    py = tpos[3 * t + 1];
-    pz = tpos[3 * t + 2];
+    px = tpos[3 * (size_t)t];
+    py = tpos[3 * (size_t)t + 1];
+    pz = tpos[3 * (size_t)t + 2];
   }
   double acc[4] = {0, 0, 0, 0};
   for (int c0 = s0; c0 < s1; c0 += NA_TILE) {
     const int cnt = min(NA_TILE, s1 - c0);
     __syncthreads();
     for (int j = threadIdx.x; j < cnt; j += blockDim.x) {
-      const int p = c0 + j;
+      const size_t p = (size_t)(c0 + j);
       sx[j] = spos[3 * p];
       sy[j] = spos[3 * p + 1];
       sz[j] = spos[3 * p + 2];
       nx[j] = snor[3 * p];
       ny[j] = snor[3 * p + 1];
       nz[j] = snor[3 * p + 2];
-      for (int s = 0; s < SD; s++) f[j * SD + s] = sden[(size_t)p * SD + s];
+      for (int s = 0; s < SD; s++) f[j * SD + s] = sden[p * SD + s];
     }
     __syncthreads();
     if (t < nt)
@@ -124,25 +120,24 @@ extern "C" kifmm_status kifmm_direct_noalloc(int kt, int ncoef, const double* co
   if (!d_trgpos || !d_trgval || (ns > 0 && (!d_srcpos || !d_srcnor || !d_srcden))) return KIFMM_ERR_ARG;
   const size_t per_chunk = (size_t)nt * td;
   if (per_chunk > (size_t)KIFMM_NOALLOC_SCRATCH_DOUBLES) return KIFMM_ERR_CAPACITY;
-  // set-up, once per device, with the device current
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NA_MAXDEV) {
+  // an error left by the caller's earlier work is reported as such (and
+  // left pending), not taken for a failure of this call's launches
+  if (cudaPeekAtLastError() != cudaSuccess) return KIFMM_ERR_CUDA;
+  int dev = 0, num_sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
     cudaGetLastError();
     return KIFMM_ERR_NO_DEVICE;
   }
+  // the scratch array's address on the current device (every call)
   double* scratch = nullptr;
   {
-    std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_scratch_ptr[dev]) {
-      void* p = nullptr;
-      cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-      if (e != cudaSuccess || !p) {
-        cudaGetLastError();
-        return KIFMM_ERR_CUDA;
-      }
-      g_scratch_ptr[dev] = (double*)p;
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
+      cudaGetLastError();
+      return KIFMM_ERR_CUDA;
     }
-    scratch = g_scratch_ptr[dev];
+    scratch = (double*)p;
   }
   cudaStream_t st = (cudaStream_t)stream;
   double kcd[3], cf[2] = {1.0, 0.25};
@@ -152,7 +147,7 @@ extern "C" kifmm_status kifmm_direct_noalloc(int kt, int ncoef, const double* co
   // chunks of sources: enough CTAs to fill the GPU, within the scratch capacity
   const int tblocks = (nt + NA_THREADS - 1) / NA_THREADS;
   int nchunk = (int)std::min<size_t>((size_t)NA_MAXCHUNK, (size_t)KIFMM_NOALLOC_SCRATCH_DOUBLES / per_chunk);
-  nchunk = std::max(1, std::min(nchunk, std::max(1, 4 * 148 / tblocks)));
+  nchunk = std::max(1, std::min(nchunk, std::max(1, 4 * num_sms / tblocks)));
   nchunk = std::max(1, std::min(nchunk, std::max(1, ns / NA_TILE)));
   const int chunk = ns > 0 ? (ns + nchunk - 1) / nchunk : 0;
   dim3 grid(tblocks, nchunk);
@@ -167,7 +162,7 @@ extern "C" kifmm_status kifmm_direct_noalloc(int kt, int ncoef, const double* co
     case 521: launch_partial<521>(grid, st, d_srcpos, d_srcnor, d_srcden, ns, chunk, d_trgpos, nt, scratch, kc); break;
   }
   const int n = (int)per_chunk;
-  k_direct_reduce<<<std::max(1, std::min((n + 255) / 256, 148 * 8)), 256, 0, st>>>(scratch, nchunk, n, d_trgval);
+  k_direct_reduce<<<std::max(1, std::min((n + 255) / 256, num_sms * 8)), 256, 0, st>>>(scratch, nchunk, n, d_trgval);
   if (cudaGetLastError() != cudaSuccess) return KIFMM_ERR_CUDA;
   return KIFMM_OK;
 }

@@ -67,6 +67,8 @@ SIGNATURES = {
     "kifmm_batch_eval_device": [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
                                 ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p, ctypes.c_int],
     "kifmm_batch_last_error": [ctypes.c_void_p],
+    "kifmm_batch_poll_status": [ctypes.c_void_p],
+    "kifmm_poll_status": [_H],
     "kifmm_status_string": [ctypes.c_int],
     "kifmm_last_error": [_H],
 }
@@ -202,6 +204,12 @@ class FMM3d:
                                                    ctypes.c_void_p(d_trgval), ctypes.c_void_p(stream),
                                                    1 if sync else 0))
 
+    def poll_status(self) -> int:
+        """Raises KifmmError(KIFMM_ERR_CUDA) if a device-side wait of an eval
+        that has completed since the last poll timed out (synchronise the
+        stream of an asynchronous eval_device first)."""
+        return self._check(lib().kifmm_poll_status(self._h))
+
     # -- FMM3d::check (fmm3d/fmm3d_check.cpp:25-73)
     def check(self, srcden, trgval, numchk: int = 20, seed: int = 0) -> float:
         srcden = np.ascontiguousarray(srcden, np.float64)
@@ -291,6 +299,13 @@ class Batch:
         src = (ctypes.c_void_p * n)(*d_srcden)
         dst = (ctypes.c_void_p * n)(*d_trgval)
         st = lib().kifmm_batch_eval_device(self._b, nrhs, src, dst, ctypes.c_void_p(stream), 1 if sync else 0)
+        if st != 0:
+            raise KifmmError(st, lib().kifmm_batch_last_error(self._b).decode())
+        return 0
+
+    def poll_status(self) -> int:
+        """kifmm_batch_poll_status: raises if an instance's device-side wait timed out."""
+        st = lib().kifmm_batch_poll_status(self._b)
         if st != 0:
             raise KifmmError(st, lib().kifmm_batch_last_error(self._b).decode())
         return 0

@@ -49,6 +49,40 @@ def imbalance(costs, parts) -> float:
     return max(loads) / mean if mean > 0 else 1.0
 
 
+def instance_cost(inst, np_: int = 6, ptsmax: int = 64) -> float:
+    """estimated_cost of one batched instance (a workloads.batched_instances
+    entry): the source dofs of its equivalent kernel weigh the V list (4 for
+    Stokes through kernel 301, 1 for Laplace)."""
+    sdof_mm = 4 if inst["kt"] in (311, 321) else 3 if inst["kt"] in (511, 521) else 1
+    return estimated_cost(inst["n"], np_, sdof_mm, ptsmax)
+
+
+def shard_instances(insts, rank: int, world: int):
+    """This rank's share of independent FMM instances: the indices of its
+    longest-processing-time part (sorted) and the partition's imbalance
+    (max rank load / mean rank load)."""
+    if not 0 <= rank < world:
+        raise ValueError("rank must be in [0, world)")
+    costs = [instance_cost(i) for i in insts]
+    parts = lpt_partition(costs, world)
+    return parts[rank], imbalance(costs, parts)
+
+
+def batched_run(insts, rank: int, world: int, run_shard, rhs: int = 1, dist=None, device=None):
+    """Evaluates a rank's share of independent instances and combines the
+    ranks' timings: run_shard(indices) sets up and times this rank's
+    instances and returns (ms per step, extra); the step time is the max over
+    ranks (no collective touches the data).  Returns a dict with the whole-job
+    Mpoints/s (every instance's points x rhs over the slowest rank's time),
+    the max time, this rank's indices, the imbalance and extra."""
+    mine, imb = shard_instances(insts, rank, world)
+    ms, extra = run_shard(mine)
+    ms = reduce_max(ms, dist, device)
+    npts = sum(int(i["n"]) for i in insts)
+    return {"value": npts * rhs / (ms / 1e3) / 1e6 if ms > 0 else float("nan"), "ms": ms, "mine": mine,
+            "imbalance": imb, "extra": extra}
+
+
 def reduce_max(value: float, dist=None, device=None) -> float:
     """Max of a float over all ranks (identity without a process group)."""
     if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:

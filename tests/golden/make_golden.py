@@ -12,7 +12,8 @@ and stores, per case:
 The reference ships no fixtures or known-answer tests of its own, so these
 are the pins for both the C restatement and the GPU engine.
 
-Usage:  python tests/golden/make_golden.py      (needs /root/reference built into oracle/_ref)
+Usage:  python tests/golden/make_golden.py      (needs the reference library oracle/_ref/libkifmm_ref.so,
+                                               built by oracle/Makefile from the reference sources)
 """
 import os
 import sys

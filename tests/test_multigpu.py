@@ -54,6 +54,54 @@ def _worker(rank, world, port, costs, out):
     dist.destroy_process_group()
 
 
+def _batched_worker(rank, world, port, out):
+    import torch.distributed as dist
+    import workloads as W
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    insts = W.batched_instances()
+    seen = []
+
+    def run_shard(mine):  # stands in for the engine: records the shard, reports a time from its cost
+        seen.extend(mine)
+        return 1e-9 * sum(multigpu.instance_cost(insts[i]) for i in mine), len(mine)
+
+    res = multigpu.batched_run(insts, rank, world, run_shard, rhs=8, dist=dist)
+    dist.barrier()
+    out[rank] = (seen, res["ms"], res["value"], res["imbalance"], res["extra"])
+    dist.destroy_process_group()
+
+
+def test_two_rank_gloo_batched_instances_are_sharded():
+    """The batched benchmark's run path (multigpu.batched_run, with the
+    engine replaced by a stand-in): on two gloo ranks every one of the 64
+    instances is evaluated by exactly one rank, the step time is the slower
+    rank's, and the value counts every instance once."""
+    import torch.multiprocessing as mp
+    import workloads as W
+    insts = W.batched_instances()
+    port = _free_port()
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as mgr:
+        out = mgr.dict()
+        procs = [ctx.Process(target=_batched_worker, args=(r, 2, port, out)) for r in range(2)]
+        for p in procs:
+            p.start()
+        for p in procs:
+            p.join(timeout=120)
+            assert p.exitcode == 0
+        res = dict(out)
+    a, b = res[0], res[1]
+    assert sorted(a[0] + b[0]) == list(range(len(insts))) and not set(a[0]) & set(b[0])
+    costs = [multigpu.instance_cost(i) for i in insts]
+    slow = max(sum(costs[i] for i in a[0]), sum(costs[i] for i in b[0])) * 1e-9
+    assert a[1] == b[1] == pytest.approx(slow)
+    npts = sum(i["n"] for i in insts)
+    assert a[2] == pytest.approx(npts * 8 / (slow / 1e3) / 1e6)
+    assert a[3] == b[3] < 1.05 and a[4] + b[4] == len(insts)
+
+
 def test_two_rank_gloo_sharding_and_max_timing():
     import torch.multiprocessing as mp
     costs = [multigpu.estimated_cost(n) for n in (10_000, 500_000, 40_000, 250_000, 90_000, 12_000, 330_000)]

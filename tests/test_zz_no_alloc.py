@@ -30,13 +30,14 @@ def existing_direct(kt, coefs, src, nor, den, trg):
     return f.direct(den, trg)
 
 
-def noalloc_direct(torch, kt, coefs, src, nor, den, trg):
-    dev = lambda a: torch.tensor(np.ascontiguousarray(a, np.float64), device="cuda")
+def noalloc_direct(torch, kt, coefs, src, nor, den, trg, stream=None):
+    dev = lambda a: torch.tensor(np.ascontiguousarray(a, np.float64).reshape(-1), device="cuda")
     d_src, d_nor, d_den, d_trg = dev(src), dev(nor), dev(den), dev(trg)
     td = kifmm.Kernel3d(kt, coefs).tdof()
     d_out = torch.full((len(trg) * td,), float("nan"), device="cuda", dtype=torch.float64)
     cf = np.ascontiguousarray(coefs, np.float64)
-    stream = torch.cuda.current_stream()
+    stream = stream or torch.cuda.current_stream()
+    torch.cuda.synchronize()  # the inputs were copied on the current stream
     st = kifmm.lib().kifmm_direct_noalloc(kt, len(cf), cf.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(src),
                                           d_src.data_ptr(), d_nor.data_ptr(), d_den.data_ptr(), len(trg),
                                           d_trg.data_ptr(), d_out.data_ptr(), stream.cuda_stream)
@@ -63,6 +64,31 @@ def test_two_calls_match_existing_direct_entry_point(gpu):
         ref = existing_direct(kt, coefs, src, nor, den, trg)
         assert np.all(np.isfinite(got))
         assert np.linalg.norm(got - ref) <= TOL * np.linalg.norm(ref)
+
+
+def test_kernels_with_two_coefficients_and_pressure_outputs(gpu):
+    """Navier single layer (two coefficients, mu and nu) and the Stokes
+    pressure kernel (three source dofs, one target dof) against kifmm_direct."""
+    torch = pytest.importorskip("torch")
+    for kt, coefs, ns, nt, seed in [(511, [1.3, 0.3], 5000, 700, 3), (312, [1.0], 6000, 500, 4)]:
+        src, nor, den, trg = case(kt, ns, nt, seed)
+        got = noalloc_direct(torch, kt, coefs, src, nor, den, trg)
+        ref = existing_direct(kt, coefs, src, nor, den, trg)
+        assert np.linalg.norm(got - ref) <= TOL * np.linalg.norm(ref)
+
+
+def test_no_sources_give_zero_potentials_on_a_side_stream(gpu):
+    """ns == 0 writes zeros over the caller's output (which starts as NaN),
+    and a call on a non-default stream is ordered on that stream."""
+    torch = pytest.importorskip("torch")
+    side = torch.cuda.Stream()
+    trg = np.random.default_rng(5).uniform(-1, 1, (300, 3))
+    got = noalloc_direct(torch, 111, [1.0], np.zeros((0, 3)), np.zeros((0, 3)), np.zeros(0), trg, stream=side)
+    assert np.array_equal(got, np.zeros(300))
+    src, nor, den, trg = case(321, 4000, 600, 6)
+    got = noalloc_direct(torch, 321, [1.0], src, nor, den, trg, stream=side)
+    ref = existing_direct(321, [1.0], src, nor, den, trg)
+    assert np.linalg.norm(got - ref) <= TOL * np.linalg.norm(ref)
 
 
 def test_request_beyond_the_fixed_scratch_is_refused(gpu):
