@@ -67,7 +67,8 @@ kifmm_status kifmm_set_box(kifmm_handle h, const double ctr[3], int rootlvl);
 
 /* One entry of the reference's option map (map<string,string>, fmm3d/tt.cpp:23-38).
  * Keys the reference requires: -<prefix>np, -<prefix>let3d_ptsmax,
- * -<prefix>let3d_maxlevel.  Engine keys: -<prefix>precision (fp64|mixed). */
+ * -<prefix>let3d_maxlevel.  Engine keys: -<prefix>precision (fp64|mixed),
+ * -<prefix>tree (device|host: where the octree and lists are built). */
 kifmm_status kifmm_set_option(kifmm_handle h, const char* key, const char* value);
 
 /* Replaces FMM3d::setup(map<string,string>&) (fmm3d/fmm3d_setup.cpp:26-63):
@@ -174,6 +175,11 @@ kifmm_status kifmm_dofs(kifmm_handle h, int* sdof, int* tdof);
  * [4] leaf (U/W/X/L2T), [5] total, and inside [1]: [6] forward spectra,
  * [7] Hadamard accumulation, [8] inverse spectra.  n = entries written. */
 kifmm_status kifmm_phase_times(kifmm_handle h, double* ms, int* n);
+/* Host wall-clock times (ms) of the last kifmm_setup: [0] octree and
+ * U/V/W/X lists (built on the GPU unless -<prefix>tree host), [1] the
+ * translation operators (cached per kernel and np), [2] device data and
+ * work lists.  n = entries written. */
+kifmm_status kifmm_setup_times(kifmm_handle h, double* ms, int* n);
 /* Enables (1) or disables (0) per-phase event timing (off by default). */
 kifmm_status kifmm_set_profiling(kifmm_handle h, int on);
 

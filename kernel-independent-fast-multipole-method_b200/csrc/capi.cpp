@@ -191,6 +191,14 @@ kifmm_status kifmm_phase_times(kifmm_handle h, double* ms, int* n) {
   return KIFMM_OK;
 }
 
+kifmm_status kifmm_setup_times(kifmm_handle h, double* ms, int* n) {
+  if (!h || !ms || !n) return KIFMM_ERR_ARG;
+  if (!h->e.tree_ready) return fail(h, KIFMM_ERR_STATE, "no setup times before setup");
+  for (int i = 0; i < 3; i++) ms[i] = h->e.setup_ms[i];
+  *n = 3;
+  return KIFMM_OK;
+}
+
 kifmm_status kifmm_set_profiling(kifmm_handle h, int on) {
   if (!h) return KIFMM_ERR_ARG;
   h->e.profiling = on != 0;

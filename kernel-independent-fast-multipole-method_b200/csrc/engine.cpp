@@ -14,6 +14,7 @@
 #include "engine.hpp"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <random>
@@ -944,9 +945,30 @@ int Engine::setup() {
     err = "kernel not supported by FMM3d";
     return KIFMM_ERR_KERNEL;
   }
+  bool tree_on_device = true;
+  {
+    auto tit = opts.find("-" + prefix + "tree");
+    if (tit != opts.end()) {
+      std::string v = tit->second;
+      v.erase(0, v.find_first_not_of(" \t"));
+      v = v.substr(0, v.find_first_of(" \t%"));
+      if (v == "host")
+        tree_on_device = false;
+      else if (v != "device") {
+        err = "tree must be device or host";
+        return KIFMM_ERR_OPTION;
+      }
+    }
+  }
   release_device();
   tree_ready = false;
-  // tree + lists
+  int ndev = 0;
+  const bool have_device = cudaGetDeviceCount(&ndev) == cudaSuccess && ndev > 0;
+  if (!have_device) cudaGetLastError();
+  // tree + lists: on the GPU (tree_gpu.cu); the host builder (tree.cpp) on
+  // request, or where there is no GPU at all -- setup then stops below with
+  // KIFMM_ERR_NO_DEVICE, and only the tree introspection is available
+  auto t0 = std::chrono::steady_clock::now();
   tree = Tree();
   tree.ctr[0] = ctr[0];
   tree.ctr[1] = ctr[1];
@@ -954,16 +976,20 @@ int Engine::setup() {
   tree.rootlvl = rootlvl;
   tree.ptsmax = ptsmax;
   tree.maxlevel = maxlevel;
-  int rc = build_tree(tree, ns, srcpos.data(), nt, trgpos.data(), host_threads(), &err);
+  int rc = (tree_on_device && have_device) ? build_tree_device(tree, ns, srcpos.data(), nt, trgpos.data(), &err)
+                                           : build_tree(tree, ns, srcpos.data(), nt, trgpos.data(), host_threads(), &err);
   if (rc == 3) return KIFMM_ERR_OUT_OF_BOX;
+  if (rc == 4) return KIFMM_ERR_CUDA;
   if (rc != 0) return KIFMM_ERR_OPTION;
   tree_ready = true;
+  auto t1 = std::chrono::steady_clock::now();
   ops = get_operators(mm, np, host_threads(), &err);
   if (!ops) return KIFMM_ERR_NUMERIC;
+  auto t2 = std::chrono::steady_clock::now();
+  setup_ms[0] = std::chrono::duration<double, std::milli>(t1 - t0).count();
+  setup_ms[1] = std::chrono::duration<double, std::milli>(t2 - t1).count();
   // device stage: there is no CPU fallback
-  int ndev = 0;
-  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
-    cudaGetLastError();
+  if (!have_device) {
     err = "no CUDA device";
     return KIFMM_ERR_NO_DEVICE;
   }
@@ -993,6 +1019,7 @@ int Engine::setup() {
     release_device();
     return e.e == cudaErrorMemoryAllocation ? KIFMM_ERR_ALLOC : KIFMM_ERR_CUDA;
   }
+  setup_ms[2] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t2).count();
   ready = true;
   return KIFMM_OK;
 }

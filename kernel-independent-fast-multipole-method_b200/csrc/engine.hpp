@@ -58,6 +58,8 @@ struct Engine {
   cudaStream_t stream = nullptr;
   // work counters (kifmm_work_counters)
   std::vector<double> counters;
+  // setup phases (ms): tree + lists, operators, device data and work lists
+  double setup_ms[3] = {0, 0, 0};
   // host-API staging (grown on demand)
   double* d_in = nullptr;
   double* d_out = nullptr;

@@ -51,4 +51,8 @@ struct Tree {
 int build_tree(Tree& t, int ns, const double* srcpos, int nt, const double* trgpos, int nthreads,
                std::string* err);
 
+// The same tree and lists built on the current GPU (tree_gpu.cu) and copied
+// into t; returns as build_tree, or 4 on a CUDA error.
+int build_tree_device(Tree& t, int ns, const double* srcpos, int nt, const double* trgpos, std::string* err);
+
 }  // namespace kifmm

@@ -60,6 +60,7 @@ SIGNATURES = {
     "kifmm_dofs": [_H, _IP, _IP],
     "kifmm_phase_times": [_H, _DP, _IP],
     "kifmm_set_profiling": [_H, ctypes.c_int],
+    "kifmm_setup_times": [_H, _DP, _IP],
     "kifmm_work_counters": [_H, _DP, _IP],
     "kifmm_last_launch_count": [_H, _IP],
     "kifmm_batch_create": [ctypes.c_int, ctypes.POINTER(_H), ctypes.POINTER(ctypes.c_void_p)],
@@ -266,6 +267,13 @@ class FMM3d:
         names = ("upward", "vlist", "xlist", "downward", "leaf", "total", "m2l_forward", "m2l_hadamard",
                  "m2l_inverse")
         return {names[i]: ms[i] for i in range(n.value)}
+
+    def setup_times(self):
+        """Host wall-clock ms of the last setup: tree + lists, operators, device build."""
+        ms = (ctypes.c_double * 8)()
+        n = ctypes.c_int()
+        self._check(lib().kifmm_setup_times(self._h, ms, ctypes.byref(n)))
+        return dict(zip(("tree_lists", "operators", "device_build"), ms[:n.value]))
 
     def work_counters(self):
         c = (ctypes.c_double * 16)()
