@@ -81,6 +81,13 @@ struct Impl : ImplBase {
     int* idx = nullptr;
     int64_t* ptr2 = nullptr;
     int* idx2 = nullptr;
+    // GEMM column lists over R density vectors: the node lists repeated
+    // with offsets r * nnodes into the [r][node][...] buffers (aux offset
+    // too when it holds node ids, copied when it holds levels)
+    std::vector<int> hw, ha;
+    bool aux_nodes = false;
+    int R = 0;
+    int *rw = nullptr, *ra = nullptr;
   };
 
   int sd_u, td_u, sd_m, td_m, nsurf, nuc;
@@ -103,7 +110,8 @@ struct Impl : ImplBase {
   int *d_sperm = nullptr, *d_tperm = nullptr, *d_path = nullptr, *d_depth = nullptr;
   T *sden = nullptr, *tval = nullptr;
   int cap_rhs = 0;
-  T *supeden, *supcval, *tdncval, *tdneden, *spectra, *effval;
+  T *supeden = nullptr, *supcval = nullptr, *tdncval = nullptr, *tdneden = nullptr, *spectra = nullptr,
+    *effval = nullptr;
   // A surface operator: row-major M x K in T (SIMT path) and, for FP32 data,
   // the split-TF32 pair for the tensor-core path.
   struct SurfOp {
@@ -258,7 +266,6 @@ struct Impl : ImplBase {
           m2l_tc16_images(nf, op.m2l.data(), &im, &isb);
           htc16_img = upload(im);
           htc16_inv_sb = upload(isb);
-          d_bound = dalloc<unsigned>(1);
         } else if (sizeof(T) == 4 && E.m2l_tc && m2l_tc_supported(nf, sd_m, td_m)) {
           std::vector<float> im;
           m2l_tc_images(nf, op.m2l.data(), &im);
@@ -280,23 +287,13 @@ struct Impl : ImplBase {
     kernel_constants(E.mm.kt, E.mm.coefs, kc);
     args.km = KConst<T>{(T)kc[0], (T)kc[1], (T)kc[2]};
     if (near64) a64.km = KConst<double>{kc[0], kc[1], kc[2]};
-    // ---- per-node data
-    supeden = dalloc<T>((size_t)nn * nsurf * sd_m);
-    KCHECK(cudaMemset(supeden, 0, sizeof(T) * (size_t)nn * nsurf * sd_m));  // empty nodes stay zero
-    supcval = dalloc<T>((size_t)nn * nuc * td_m);
-    tdncval = dalloc<T>((size_t)nn * nsurf * td_m);
-    tdneden = dalloc<T>((size_t)nn * nsurf * sd_m);
-    KCHECK(cudaMemset(tdneden, 0, sizeof(T) * (size_t)nn * nsurf * sd_m));
-    // y of a source-free child stays zero; z of a target-free child is written
-    // by the L2L chain but never read
-    ybuf = dalloc<T>((size_t)nn * ru);
-    KCHECK(cudaMemset(ybuf, 0, sizeof(T) * (size_t)nn * ru));
-    zbuf = dalloc<T>((size_t)nn * rd);
-    KCHECK(cudaMemset(zbuf, 0, sizeof(T) * (size_t)nn * rd));
-    args.supeden = supeden;
-    args.supcval = supcval;
-    args.tdncval = tdncval;
-    args.tdneden = tdneden;
+    // ---- per-node data: allocated per chunk of density vectors (ensure_chunk)
+    S_supe = (size_t)nn * nsurf * sd_m;
+    S_supc = (size_t)nn * nuc * td_m;
+    S_tdnc = (size_t)nn * nsurf * td_m;
+    S_tdne = (size_t)nn * nsurf * sd_m;
+    S_y = (size_t)nn * ru;
+    S_z = (size_t)nn * rd;
 
     // ---- work lists
     const int md = tr.maxdepth;
@@ -322,6 +319,12 @@ struct Impl : ImplBase {
           }
       up_non[d] = make_list(un, unc);
       dn_par[d] = make_list(dp, dpc);
+      up_non[d].hw = un;
+      up_non[d].ha = unc;
+      up_non[d].aux_nodes = true;
+      dn_par[d].hw = dp;
+      dn_par[d].ha = dpc;
+      dn_par[d].aux_nodes = true;
     }
     {
       // all-level lists (aux = node depth): source leaves, every upward node,
@@ -343,6 +346,12 @@ struct Impl : ImplBase {
       s2m = make_list(v_s2m, s2m_lvl);
       up_all = make_list(all_up, all_up_lvl);
       dn_all = make_list(all_dn, all_dn_lvl);
+      s2m.hw = v_s2m;
+      s2m.ha = s2m_lvl;
+      up_all.hw = all_up;
+      up_all.ha = all_up_lvl;
+      dn_all.hw = all_dn;
+      dn_all.ha = all_dn_lvl;
       KCHECK(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, E.device));
       gemm_ws_len = (size_t)4 << 20;  // split-K slices of the shallow levels (32 MB)
       gemm_ws = dalloc<double>(gemm_ws_len);
@@ -369,14 +378,12 @@ struct Impl : ImplBase {
         if (mark[g]) fwdn.push_back(g);
       m2l = make_list(work, {}, ptr, idx);
       fwd = make_list(fwdn, {});
-      effval = dalloc<T>((size_t)((nn + 15) / 8 * 8) * td_m * op.nfc * 2);  // room for the sibling-group layout
+      S_eff = (size_t)((nn + 15) / 8 * 8) * td_m * op.nfc * 2;  // room for the sibling-group layout
       // nn + 8 blocks: nodes outside every V list keep a zero spectrum, and the
       // 8 blocks from index nn on stand for an absent colleague (parent-pair form)
       // (tensor-core form: sibling-group major, node n in group (n + 7) / 8,
       // the zero block a group of its own: (nn + 15) / 8 groups of 8 nodes)
-      const size_t spec_len = std::max((size_t)(nn + 8) * sd_m, htc() ? (size_t)(nn + 15) / 8 * 8 : 0) * op.nfc * 2;
-      spectra = dalloc<T>(spec_len);
-      KCHECK(cudaMemset(spectra, 0, sizeof(T) * spec_len));
+      S_spec = std::max((size_t)(nn + 8) * sd_m, htc() ? (size_t)(nn + 15) / 8 * 8 : 0) * op.nfc * 2;
       counters_v = (double)idx.size();
       if (ktiles || ttiles || htc()) build_pairs(work);
       counters_fwd = (double)fwdn.size();
@@ -461,6 +468,10 @@ struct Impl : ImplBase {
     counters_gemm = gf;
     for (auto& x : ev) KCHECK(cudaEventCreate(&x));
     have_events = true;
+    // density vectors per pass: as many as fit 8 GB of per-vector node data,
+    // at most 8 (the spectra are one set, reused vector by vector)
+    const double per_rhs = (double)sizeof(T) * (S_supe + S_supc + S_tdnc + S_tdne + S_y + S_z);
+    max_chunk = (int)std::max(1.0, std::min(8.0, std::floor(8e9 / std::max(per_rhs, 1.0))));
     ensure_rhs(1);
   }
 
@@ -639,7 +650,59 @@ struct Impl : ImplBase {
     return l;
   }
 
+  size_t S_supe = 0, S_supc = 0, S_tdnc = 0, S_tdne = 0, S_y = 0, S_z = 0, S_spec = 0, S_eff = 0;
+  int cap_chunk = 0, max_chunk = 1;
+
+  void replicate(List& L, int R) {
+    if (L.n <= 0 || L.R >= R) return;
+    const int nn = tr.nnodes;
+    std::vector<int> w((size_t)R * L.n), a;
+    if (!L.ha.empty()) a.resize((size_t)R * L.n);
+    for (int r = 0; r < R; r++)
+      for (int j = 0; j < L.n; j++) {
+        w[(size_t)r * L.n + j] = L.hw[j] + r * nn;
+        if (!a.empty()) a[(size_t)r * L.n + j] = L.ha[j] + (L.aux_nodes ? r * nn : 0);
+      }
+    L.rw = upload(w);
+    L.ra = a.empty() ? nullptr : upload(a);
+    L.R = R;
+  }
+
+  // per-vector node data for R density vectors at once, [r][node][...]
+  void ensure_chunk(int R) {
+    if (R <= cap_chunk) return;
+    supeden = dalloc<T>((size_t)R * S_supe);
+    KCHECK(cudaMemset(supeden, 0, sizeof(T) * (size_t)R * S_supe));  // empty nodes stay zero
+    supcval = dalloc<T>((size_t)R * S_supc);
+    tdncval = dalloc<T>((size_t)R * S_tdnc);
+    tdneden = dalloc<T>((size_t)R * S_tdne);
+    KCHECK(cudaMemset(tdneden, 0, sizeof(T) * (size_t)R * S_tdne));
+    // y of a source-free child stays zero; z of a target-free child is written
+    // by the L2L chain but never read
+    ybuf = dalloc<T>((size_t)R * S_y);
+    KCHECK(cudaMemset(ybuf, 0, sizeof(T) * (size_t)R * S_y));
+    zbuf = dalloc<T>((size_t)R * S_z);
+    KCHECK(cudaMemset(zbuf, 0, sizeof(T) * (size_t)R * S_z));
+    if (!spectra && S_spec) {  // one set: the V list runs vector by vector
+      spectra = dalloc<T>(S_spec);
+      KCHECK(cudaMemset(spectra, 0, sizeof(T) * S_spec));
+      effval = dalloc<T>(S_eff);
+    }
+    if (htc16_img) d_bound = dalloc<unsigned>(R);
+    args.supeden = supeden;
+    args.supcval = supcval;
+    args.tdncval = tdncval;
+    args.tdneden = tdneden;
+    replicate(s2m, R);
+    replicate(up_all, R);
+    replicate(dn_all, R);
+    for (auto& L : up_non) replicate(L, R);
+    for (auto& L : dn_par) replicate(L, R);
+    cap_chunk = R;
+  }
+
   void ensure_rhs(int nrhs) {
+    ensure_chunk(std::min(nrhs, max_chunk));
     if (nrhs <= cap_rhs) return;
     sden = dalloc<T>((size_t)nrhs * E.ns * sd_u);
     tval = dalloc<T>((size_t)nrhs * E.nt * td_u);
@@ -672,7 +735,9 @@ struct Impl : ImplBase {
                                    num_sms, st);
   }
 
-  void p2p(const List& l, int which, int rhs, cudaStream_t st) {
+  // a P2P pass for density vector rhs (global index, selects the sorted
+  // densities and potentials) on slice r of the per-vector node data
+  void p2p(const List& l, int which, int rhs, int r, cudaStream_t st) {
     if (l.n <= 0) return;
     P2PWork w;
     w.work = l.work;
@@ -681,16 +746,67 @@ struct Impl : ImplBase {
     w.idx = l.idx;
     w.ptr2 = l.ptr2;
     w.idx2 = l.idx2;
-    launch_p2p<T>(E.user.kt, args, w, which, rhs, st);
+    P2PArgs<T> a = args;
+    a.supeden = supeden + (size_t)r * S_supe;
+    a.supcval = supcval + (size_t)r * S_supc;
+    a.tdncval = tdncval + (size_t)r * S_tdnc;
+    a.tdneden = tdneden + (size_t)r * S_tdne;
+    launch_p2p<T>(E.user.kt, a, w, which, rhs, st);
     nlaunch++;
   }
 
+  // the V list for density vector slice r: forward spectra, Hadamard, inverse
+  void vlist(int r, bool prof, cudaStream_t st) {
+    T* sup = supeden + (size_t)r * S_supe;
+    T* spec = spectra;  // reused by every vector of the chunk, in stream order
+    T* eff = effval;
+    T* tdc = tdncval + (size_t)r * S_tdnc;
+    M2LGeom g = geom;
+    if constexpr (sizeof(T) == 4) {
+      if (htc16_img) {  // the largest value a spectrum can hold, for the FP16 scale
+        g.bound = d_bound + r;
+        launch_spectra_bound(sup, fwd.work, fwd.n, d_depth, E.rootlvl, op.deg[0], nsurf, d_bound + r, num_sms, st);
+        nlaunch++;
+      }
+    }
+    launch_m2l_forward<T>(g, sup, fwd.work, fwd.n, d_depth, spec, st);
+    if (prof) KCHECK(cudaEventRecord(ev[7], st));
+    if (pairs_n > 0 && htc16_img) {
+      launch_m2l_hadamard_tc16(E.had_groups, op.nfc, htc16_img, reinterpret_cast<const unsigned*>(spec), pairs_n,
+                               pairs_chd, htc16_ctab, htc_dirs, reinterpret_cast<float*>(eff), d_bound + r,
+                               htc16_inv_sb, E.wait_limit, d_status, num_sms, st);
+      KCHECK(cudaGetLastError());
+    } else if (pairs_n > 0 && htc_img) {
+      launch_m2l_hadamard_tc(op.nfc, htc_img, reinterpret_cast<const float*>(spec), pairs_n, pairs_chd, pairs_coll,
+                             pairs_mask, htc_dirs, reinterpret_cast<float*>(eff), tr.nnodes, d_status, num_sms, st);
+      KCHECK(cudaGetLastError());
+    } else if (pairs_n > 0) {
+      if (ttiles)
+        launch_m2l_hadamard_tz<T>(op.nfc, sd_m, td_m, ttiles, spec, pairs_n, pairs_chd, pairs_coll, pairs_mask, eff,
+                                  tr.nnodes, d_status, num_sms, st);
+      else
+        launch_m2l_hadamard_sweep<T>(op.nfc, sd_m, td_m, ktiles, spec, pairs_n, pairs_chd, pairs_coll, pairs_mask,
+                                     eff, tr.nnodes, d_status, num_sms, st);
+    } else {
+      launch_m2l_hadamard<T>(g, khat, spec, m2l.work, m2l.n, m2l.ptr, m2l.idx, d_path, eff, st);
+    }
+    if (prof) KCHECK(cudaEventRecord(ev[8], st));
+    launch_m2l_inverse<T>(g, eff, m2l.work, m2l.n, tdc, st);
+    nlaunch += 2 + (pairs_n > 0 ? (htc() ? 1 : sd_m * td_m) : 1);
+  }
+
+  // Density vectors go through the passes in chunks of up to max_chunk: the
+  // point-surface passes and the V list run once per vector, and every
+  // surface contraction runs once per chunk over all of its vectors' nodes
+  // (the node lists repeated with offsets into [r][node][...] buffers), so
+  // the operator is read once for the whole chunk.
   int eval(const double* d_srcden, double* d_trgval, int nrhs, cudaStream_t st) override {
     ensure_rhs(nrhs);
     nlaunch = 0;
     const int md = tr.maxdepth;
     const int K1 = nsurf * sd_m;
-    bool prof = E.profiling;
+    const int chunk = std::max(1, std::min(nrhs, cap_chunk));
+    const bool prof = E.profiling && nrhs <= chunk;  // phase events for a single chunk
     if (prof) KCHECK(cudaEventRecord(ev[0], st));
     launch_scatter_den<T>(d_srcden, d_sperm, E.ns, sd_u, nrhs, sden, st);
     nlaunch++;
@@ -698,81 +814,53 @@ struct Impl : ImplBase {
       launch_scatter_den<double>(d_srcden, d_sperm, E.ns, sd_u, nrhs, sden64, st);
       nlaunch++;
     }
-    for (int r = 0; r < nrhs; r++) {
-      // upward
-      p2p(s2m, P2P_S2M, r, st);
-      // y = up_W * check on the leaves of every level at once, M2M bottom-up
-      // in y coordinates, then every node's density = 2^(-l deg) up_V * y
-      gemm(op_upW, supcval, (int64_t)nuc * td_m, s2m.work, ybuf, ru, s2m.work, s2m.n, false, st);
+    for (int r0 = 0; r0 < nrhs; r0 += chunk) {
+      const int R = std::min(chunk, nrhs - r0);
+      // upward: S2M per vector, then y = up_W * check on the leaves of every
+      // level and vector at once, M2M bottom-up in y coordinates, and every
+      // node's density = 2^(-l deg) up_V * y
+      for (int r = 0; r < R; r++) p2p(s2m, P2P_S2M, r0 + r, r, st);
+      gemm(op_upW, supcval, (int64_t)nuc * td_m, s2m.rw, ybuf, ru, s2m.rw, R * s2m.n, false, st);
       for (int d = md - 1; d >= 2; d--) {
         const List& P = up_non[d];
-        gemm(op_m2my, ybuf, ru, P.aux, ybuf, ru, P.work, P.n, false, st);
+        gemm(op_m2my, ybuf, ru, P.ra, ybuf, ru, P.rw, R * P.n, false, st);
       }
-      gemm(op_upV, ybuf, ru, up_all.work, supeden, K1, up_all.work, up_all.n, false, st, up_all.aux);
-      if (prof && r == 0) KCHECK(cudaEventRecord(ev[1], st));
+      gemm(op_upV, ybuf, ru, up_all.rw, supeden, K1, up_all.rw, R * up_all.n, false, st, up_all.ra);
+      if (prof) KCHECK(cudaEventRecord(ev[1], st));
       // V list
-      KCHECK(cudaMemsetAsync(tdncval, 0, sizeof(T) * (size_t)tr.nnodes * nsurf * td_m, st));
-      if (m2l.n > 0) {
-        if constexpr (sizeof(T) == 4) {
-          if (htc16_img) {  // the largest value a spectrum can hold, for the FP16 scale
-            launch_spectra_bound(supeden, fwd.work, fwd.n, d_depth, E.rootlvl, op.deg[0], nsurf, d_bound, num_sms, st);
-            nlaunch++;
-          }
-        }
-        launch_m2l_forward<T>(geom, supeden, fwd.work, fwd.n, d_depth, spectra, st);
-        if (prof && r == 0) KCHECK(cudaEventRecord(ev[7], st));
-        if (pairs_n > 0 && htc16_img) {
-          launch_m2l_hadamard_tc16(E.had_groups, op.nfc, htc16_img, reinterpret_cast<const unsigned*>(spectra),
-                                   pairs_n, pairs_chd, htc16_ctab, htc_dirs, reinterpret_cast<float*>(effval), d_bound,
-                                   htc16_inv_sb, E.wait_limit, d_status, num_sms, st);
-          KCHECK(cudaGetLastError());
-        } else if (pairs_n > 0 && htc_img) {
-          launch_m2l_hadamard_tc(op.nfc, htc_img, reinterpret_cast<const float*>(spectra), pairs_n, pairs_chd,
-                                 pairs_coll, pairs_mask, htc_dirs, reinterpret_cast<float*>(effval), tr.nnodes,
-                                 d_status, num_sms, st);
-          KCHECK(cudaGetLastError());
-        } else if (pairs_n > 0)
-          if (ttiles)
-            launch_m2l_hadamard_tz<T>(op.nfc, sd_m, td_m, ttiles, spectra, pairs_n, pairs_chd, pairs_coll, pairs_mask,
-                                      effval, tr.nnodes, d_status, num_sms, st);
-          else
-            launch_m2l_hadamard_sweep<T>(op.nfc, sd_m, td_m, ktiles, spectra, pairs_n, pairs_chd, pairs_coll,
-                                         pairs_mask, effval, tr.nnodes, d_status, num_sms, st);
-        else
-          launch_m2l_hadamard<T>(geom, khat, spectra, m2l.work, m2l.n, m2l.ptr, m2l.idx, d_path, effval, st);
-        if (prof && r == 0) KCHECK(cudaEventRecord(ev[8], st));
-        launch_m2l_inverse<T>(geom, effval, m2l.work, m2l.n, tdncval, st);
-        nlaunch += 2 + (pairs_n > 0 ? sd_m * td_m : 1);
-      }
-      if (prof && r == 0) KCHECK(cudaEventRecord(ev[2], st));
+      KCHECK(cudaMemsetAsync(tdncval, 0, sizeof(T) * (size_t)R * S_tdnc, st));
+      if (m2l.n > 0)
+        for (int r = 0; r < R; r++) vlist(r, prof && r == 0, st);
+      if (prof) KCHECK(cudaEventRecord(ev[2], st));
       // X list
-      p2p(s2l, P2P_S2L, r, st);
-      if (prof && r == 0) KCHECK(cudaEventRecord(ev[3], st));
-      // downward
-      // z = dn_W * check on the target nodes of every level at once, L2L
-      // top-down in z coordinates into the 8 children, then every node's
-      // density = 2^(-l deg) dn_V * z
-      gemm(op_dnW, tdncval, (int64_t)nsurf * td_m, dn_all.work, zbuf, rd, dn_all.work, dn_all.n, false, st);
+      for (int r = 0; r < R; r++) p2p(s2l, P2P_S2L, r0 + r, r, st);
+      if (prof) KCHECK(cudaEventRecord(ev[3], st));
+      // downward: z = dn_W * check on the target nodes of every level and
+      // vector at once, L2L top-down in z coordinates into the 8 children,
+      // then every node's density = 2^(-l deg) dn_V * z
+      gemm(op_dnW, tdncval, (int64_t)nsurf * td_m, dn_all.rw, zbuf, rd, dn_all.rw, R * dn_all.n, false, st);
       for (int d = 3; d <= md; d++) {
         const List& P = dn_par[d];
-        gemm(op_l2lz, zbuf, rd, P.work, zbuf, rd, P.aux, P.n, true, st);
+        gemm(op_l2lz, zbuf, rd, P.rw, zbuf, rd, P.ra, R * P.n, true, st);
       }
-      gemm(op_dnV, zbuf, rd, dn_all.work, tdneden, K1, dn_all.work, dn_all.n, false, st, dn_all.aux);
-      if (prof && r == 0) KCHECK(cudaEventRecord(ev[4], st));
+      gemm(op_dnV, zbuf, rd, dn_all.rw, tdneden, K1, dn_all.rw, R * dn_all.n, false, st, dn_all.ra);
+      if (prof) KCHECK(cudaEventRecord(ev[4], st));
       // leaves
-      p2p(leaf, P2P_LEAF, r, st);
-      if (near64 && near_u.n > 0) {
-        P2PWork w;
-        w.work = near_u.work;
-        w.n = near_u.n;
-        w.ptr = near_u.ptr;
-        w.idx = near_u.idx;
-        w.ptr2 = near_u.ptr2;
-        w.idx2 = near_u.idx2;
-        launch_p2p<double>(E.user.kt, a64, w, P2P_LEAF, r, st);
-        nlaunch++;
+      for (int r = 0; r < R; r++) {
+        p2p(leaf, P2P_LEAF, r0 + r, r, st);
+        if (near64 && near_u.n > 0) {
+          P2PWork w;
+          w.work = near_u.work;
+          w.n = near_u.n;
+          w.ptr = near_u.ptr;
+          w.idx = near_u.idx;
+          w.ptr2 = near_u.ptr2;
+          w.idx2 = near_u.idx2;
+          launch_p2p<double>(E.user.kt, a64, w, P2P_LEAF, r0 + r, st);
+          nlaunch++;
+        }
       }
-      if (prof && r == 0) KCHECK(cudaEventRecord(ev[5], st));
+      if (prof) KCHECK(cudaEventRecord(ev[5], st));
     }
     if constexpr (sizeof(T) == 4) {
       if (near64)
@@ -794,7 +882,7 @@ struct Impl : ImplBase {
       KCHECK(cudaEventElapsedTime(&ms, ev[0], ev[6]));
       pt[5] = ms;
       if (m2l.n > 0) {
-        // ev[1] -> memset -> fwd -> ev[7] -> hadamard -> ev[8] -> inverse -> ev[2]
+        // ev[1] -> memset -> fwd -> ev[7] -> hadamard -> ev[8] -> inverse (vector 0) ...
         KCHECK(cudaEventElapsedTime(&ms, ev[1], ev[7]));
         pt[6] = ms;
         KCHECK(cudaEventElapsedTime(&ms, ev[7], ev[8]));

@@ -52,11 +52,16 @@ def test_batch_matches_single_instance_evals(gpu):
         b.eval([s.data_ptr() for s in srcs], [o.data_ptr() for o in outs], nrhs, 0, sync=True)
         for o, w in zip(outs, want):
             assert np.array_equal(o.cpu().numpy(), w)
-    # other buffers and a single rhs: recaptured
+    # other buffers and a single rhs: recaptured.  One density vector alone
+    # runs the surface contractions over half the columns of the two-vector
+    # pass, so the split-K schedule (and the FP32 summation order) may differ:
+    # equal to rounding, 1e-13 relative in FP64 and 1e-6 in mixed precision
     outs1 = [torch.zeros(o.numel() // nrhs, device="cuda", dtype=torch.float64) for o in outs]
     b.eval([s.data_ptr() for s in srcs], [o.data_ptr() for o in outs1], 1, 0, sync=True)
-    for o, w in zip(outs1, want):
-        assert np.array_equal(o.cpu().numpy(), w[: o.numel()])
+    for (name, prec), o, w in zip(cases, outs1, want):
+        got, ref = o.cpu().numpy(), w[: o.numel()]
+        tol = 1e-13 if prec == "fp64" else 1e-6
+        assert np.linalg.norm(got - ref) <= tol * np.linalg.norm(ref), name
 
 
 def test_batch_rejects_bad_arguments(gpu):
