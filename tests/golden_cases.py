@@ -2,6 +2,8 @@
 
 * ``<name>.npz``      small cases with full inputs, outputs, tree and lists
                       (made by tests/golden/make_golden.py);
+* ``batched_stokes_ref.npz``  the reference's own errors on the batched
+                      workload's Stokes instances (tests/golden/make_batched_golden.py);
 * ``cfg_<name>.npz``  the benchmark configurations at full size: reference
                       output and direct sum at the check targets only; the
                       inputs are regenerated from their seeds by workloads.py
@@ -17,7 +19,7 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 def names():
     return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz"))
-                  if not os.path.basename(p).startswith("cfg_"))
+                  if not os.path.basename(p).startswith(("cfg_", "batched_")))
 
 
 def load(name):

@@ -16,6 +16,8 @@ The CPU tests check that the regenerated inputs are the fixture's inputs
 (checksums) and that the oracle's direct sum reproduces the reference's at
 the check targets to 1e-12.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -96,3 +98,34 @@ def test_mixed_engine_matches_reference_at_size(gpu, name):
     got = run_engine(d, "mixed")
     err = oracle.relerr(got, d["ref_direct"])
     assert err <= max(FP64_FACTOR * d["ref_relerr"], MIXED_FLOOR), (err, d["ref_relerr"])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batched_stokes_instance_matches_reference_error(gpu, precision):
+    """The batched workload's largest-error Stokes instance (index 11: 75,496
+    points of the Plummer ball, kernel 311, np=6, 8 density vectors in one
+    pass) against the reference's own error on it, for density vectors 0 and
+    7 (tests/golden/batched_stokes_ref.npz): within 10x, and the bench's
+    per-instance bound max(1e-5, 10 x the reference)."""
+    import kifmm
+    z = np.load(os.path.join(G.GOLDEN, "batched_stokes_ref.npz"))
+    ref = dict(zip(z["index"].tolist(), z["ref_relerr"].tolist()))
+    inst = W.batched_instances()[11]
+    n, rhs = inst["n"], 8
+    p, _ = W.GEOMETRIES[inst["geometry"]](n, inst["seed"])
+    den = W.densities(n * rhs, 3, "uniform", inst["seed"] + 1)
+    f = kifmm.FMM3d("fmm3d_")
+    f.srcpos = f.srcnor = f.trgpos = p
+    f.knl = kifmm.Kernel3d(inst["kt"], list(inst["coefs"]))
+    f.setup({"-fmm3d_np": "6", "-fmm3d_let3d_ptsmax": "64", "-fmm3d_let3d_maxlevel": "10",
+             "-fmm3d_precision": precision})
+    out = np.zeros((rhs, 3 * n))
+    f.eval_multi(den.reshape(rhs, 3 * n), out)
+    chk = W.check_indices(n, 256, inst["seed"] + 2)
+    for k, r in enumerate((0, rhs - 1)):
+        dr = den[r * n * 3:(r + 1) * n * 3]
+        direct = f.direct(dr, p[chk]).reshape(-1, 3)
+        got = out[r].reshape(-1, 3)[chk]
+        err = oracle.relerr(got, direct)
+        assert err <= 10 * ref[11][k], (r, err, ref[11][k])
