@@ -314,7 +314,7 @@ def batched_section(torch, kifmm, stream, flush, steps, warmup, precision, pg=No
 
     def run_shard(mine):
         insts = [insts_all[i] for i in mine]
-        fmms, srcs, outs, dens, pts = [], [], [], [], []
+        fmms, srcs, outs, dens, pts, scheds = [], [], [], [], [], []
         t0 = time.perf_counter()
         for inst in insts:
             p, _ = W.GEOMETRIES[inst["geometry"]](inst["n"], inst["seed"])
@@ -323,7 +323,12 @@ def batched_section(torch, kifmm, stream, flush, steps, warmup, precision, pg=No
             f.knl = kifmm.Kernel3d(inst["kt"], list(inst["coefs"]))
             o = dict(OPTS)
             o["-fmm3d_precision"] = precision
+            # schedule autotuned at setup for 8 density vectors (cached per
+            # kernel, np, precision and tree size class across instances)
+            o["-fmm3d_autotune"] = "1"
+            o["-fmm3d_autotune_rhs"] = str(BATCH_RHS)
             f.setup(o)
+            scheds.append(f.schedule())
             sd, td = W.KERNEL_DOFS[inst["kt"]]
             den = W.densities(inst["n"] * BATCH_RHS, sd, "uniform", inst["seed"] + 1)
             fmms.append(f)
@@ -368,7 +373,13 @@ def batched_section(torch, kifmm, stream, flush, steps, warmup, precision, pg=No
                 # FMM3d::check's metric (fmm3d/fmm3d_check.cpp:61-69): ||fmm - direct|| / ||fmm||
                 errs.append((float(np.linalg.norm(direct - got) / np.linalg.norm(got)), inst["index"], r))
         del b
-        return statistics.mean(times), {"errs": errs, "setup_s": setup_s, "launches": launches}
+        tuned = {}
+        for inst, sc in zip(insts, scheds):
+            k = f'{inst["kt"]}:g{sc["had_groups"]}:c{sc["rhs_chunk"]}'
+            tuned[k] = tuned.get(k, 0) + 1
+        return statistics.mean(times), {"errs": errs, "setup_s": setup_s, "launches": launches,
+                                        "schedules": tuned,
+                                        "tuned_fresh": sum(1 for sc in scheds if not sc["from_cache"])}
 
     res = multigpu.batched_run(insts_all, rank, world, run_shard, rhs=BATCH_RHS, dist=pg,
                                device=torch.device("cuda"))
@@ -399,6 +410,7 @@ def batched_section(torch, kifmm, stream, flush, steps, warmup, precision, pg=No
             "outside_bound": outside, "bound": "max(1e-5, 10 x the reference's error on the instance)",
             "max_ratio_to_reference_error": ratio,
             "setup_s": extra["setup_s"], "launches_per_step": extra["launches"],
+            "autotuned_schedules": extra["schedules"], "schedules_tuned_fresh": extra["tuned_fresh"],
             "points_per_instance_total": sum(i["n"] for i in insts_all), "instances_this_rank": len(res["mine"]),
             "lpt_imbalance": res["imbalance"]}
 
@@ -467,6 +479,7 @@ def engine_arm(args):
         f.knl = kifmm.Kernel3d(111, [1.0])
         o = dict(OPTS)
         o["-fmm3d_precision"] = prec
+        o["-fmm3d_autotune"] = "1"  # schedule timed at setup, the fastest kept
         t0 = time.perf_counter()
         f.setup(o)
         return f, time.perf_counter() - t0
@@ -510,6 +523,8 @@ def engine_arm(args):
 
     # ---- mixed (headline)
     fm, setup_mixed = make("mixed")
+    sched_mixed = fm.schedule()
+    setup_phases = fm.setup_times()
     clocks = ClockSampler(local)
     clocks.start()
     ms_mixed, _ = timed(fm, args.steps, args.warmup)
@@ -623,6 +638,8 @@ def engine_arm(args):
         "phases_ms": phases,
         "work": wc,
         "setup_s": setup_mixed,
+        "setup_phases_ms": setup_phases,
+        "schedule": sched_mixed,
         "roofline": had_roof,
         "clocks": clk,
         "cpu_baseline": cpu,

@@ -68,7 +68,12 @@ kifmm_status kifmm_set_box(kifmm_handle h, const double ctr[3], int rootlvl);
 /* One entry of the reference's option map (map<string,string>, fmm3d/tt.cpp:23-38).
  * Keys the reference requires: -<prefix>np, -<prefix>let3d_ptsmax,
  * -<prefix>let3d_maxlevel.  Engine keys: -<prefix>precision (fp64|mixed),
- * -<prefix>tree (device|host: where the octree and lists are built). */
+ * -<prefix>tree (device|host: where the octree and lists are built),
+ * -<prefix>m2l_form (tensor|tensor_tf32|toeplitz|direct: the V-list
+ * Hadamard's form), -<prefix>tensor_cores (0|1), -<prefix>wait_limit,
+ * -<prefix>had_groups (2|3), -<prefix>rhs_chunk (0..8), -<prefix>autotune
+ * (0|1) and -<prefix>autotune_rhs (1..64): see kifmm_poll_status and
+ * kifmm_schedule. */
 kifmm_status kifmm_set_option(kifmm_handle h, const char* key, const char* value);
 
 /* Replaces FMM3d::setup(map<string,string>&) (fmm3d/fmm3d_setup.cpp:26-63):
@@ -178,8 +183,20 @@ kifmm_status kifmm_phase_times(kifmm_handle h, double* ms, int* n);
 /* Host wall-clock times (ms) of the last kifmm_setup: [0] octree and
  * U/V/W/X lists (built on the GPU unless -<prefix>tree host), [1] the
  * translation operators (cached per kernel and np), [2] device data and
- * work lists.  n = entries written. */
+ * work lists, [3] schedule autotuning (-<prefix>autotune 1).  n = entries
+ * written. */
 kifmm_status kifmm_setup_times(kifmm_handle h, double* ms, int* n);
+/* The evaluation schedule in use (no counterpart in the reference, whose
+ * eval has a single fixed schedule): [0] producer warp groups of the FP16
+ * tensor-core V-list Hadamard (2 or 3), [1] density vectors carried by one
+ * pass of the surface contractions (0: as many as fit, at most 8), [2] 1 if
+ * setup autotuned them (-<prefix>autotune 1: every candidate timed on
+ * -<prefix>autotune_rhs synthetic density vectors, the fastest kept), [3] 1
+ * if the choice came from the process-wide cache of an earlier setup with
+ * the same kernel, np, precision, V-list form, tree size class and vector
+ * count, [4] candidates timed, [5] the best candidate's ms per eval.
+ * n = entries written (6). */
+kifmm_status kifmm_schedule(kifmm_handle h, double* values, int* n);
 /* Enables (1) or disables (0) per-phase event timing (off by default). */
 kifmm_status kifmm_set_profiling(kifmm_handle h, int on);
 

@@ -194,8 +194,16 @@ kifmm_status kifmm_phase_times(kifmm_handle h, double* ms, int* n) {
 kifmm_status kifmm_setup_times(kifmm_handle h, double* ms, int* n) {
   if (!h || !ms || !n) return KIFMM_ERR_ARG;
   if (!h->e.tree_ready) return fail(h, KIFMM_ERR_STATE, "no setup times before setup");
-  for (int i = 0; i < 3; i++) ms[i] = h->e.setup_ms[i];
-  *n = 3;
+  for (int i = 0; i < 4; i++) ms[i] = h->e.setup_ms[i];
+  *n = 4;
+  return KIFMM_OK;
+}
+
+kifmm_status kifmm_schedule(kifmm_handle h, double* values, int* n) {
+  if (!h || !values || !n) return KIFMM_ERR_ARG;
+  if (!h->e.ready) return fail(h, KIFMM_ERR_STATE, "no schedule before setup");
+  for (int i = 0; i < 6; i++) values[i] = h->e.schedule[i];
+  *n = 6;
   return KIFMM_OK;
 }
 

@@ -17,8 +17,10 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <random>
 #include <thread>
+#include <tuple>
 
 #include "../../include/kifmm.h"
 #include "launch.hpp"
@@ -42,6 +44,49 @@ struct CudaError {
     cudaError_t _e = (call);                              \
     if (_e != cudaSuccess) throw CudaError{_e, #call};    \
   } while (0)
+
+// The FP16 operator images of the tensor-core Hadamard on one device, shared
+// by every engine whose translation operators are the same object (the
+// operator cache hands one object per kernel and np to every engine): the
+// images of a multi-dof kernel reach hundreds of MB (Stokes np=6: 217 chunks
+// x 26 directions x 12 dof pairs x 4 KB), so instances of a batch keep one
+// copy.  Freed with the last engine that holds them.
+struct Tc16Images {
+  unsigned short* img = nullptr;
+  float* inv_sb = nullptr;
+  int device = 0;
+  ~Tc16Images() {
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != device) cudaSetDevice(device);
+    if (img) cudaFree(img);
+    if (inv_sb) cudaFree(inv_sb);
+    if (cur != device) cudaSetDevice(cur);
+  }
+};
+
+std::shared_ptr<Tc16Images> tc16_images(const std::shared_ptr<const Operators>& ops, int device, int nf, int sd,
+                                        int td) {
+  static std::mutex mu;
+  static std::map<std::pair<const Operators*, int>, std::pair<std::weak_ptr<const Operators>, std::weak_ptr<Tc16Images>>>
+      cache;
+  std::lock_guard<std::mutex> lk(mu);
+  const auto key = std::make_pair(ops.get(), device);
+  auto it = cache.find(key);
+  if (it != cache.end() && !it->second.first.expired())
+    if (auto p = it->second.second.lock()) return p;
+  std::vector<unsigned short> im;
+  std::vector<float> isb;
+  m2l_tc16_images(nf, sd, td, ops->m2l.data(), &im, &isb);
+  auto p = std::make_shared<Tc16Images>();
+  p->device = device;
+  KCHECK(cudaMalloc(&p->img, im.size() * sizeof(unsigned short)));
+  KCHECK(cudaMemcpy(p->img, im.data(), im.size() * sizeof(unsigned short), cudaMemcpyHostToDevice));
+  KCHECK(cudaMalloc(&p->inv_sb, isb.size() * sizeof(float)));
+  KCHECK(cudaMemcpy(p->inv_sb, isb.data(), isb.size() * sizeof(float), cudaMemcpyHostToDevice));
+  cache[key] = std::make_pair(std::weak_ptr<const Operators>(ops), std::weak_ptr<Tc16Images>(p));
+  return p;
+}
 
 }  // namespace
 
@@ -127,7 +172,8 @@ struct Impl : ImplBase {
   T* ktiles = nullptr;  // [td][sd][ceil(nf/32)][343][32] operator spectra for the parent-pair sweep
   T* ttiles = nullptr;  // [td][sd][ceil(nf/16)][26][27][16] Toeplitz-factored operator
   float* htc_img = nullptr;         // tensor-core Hadamard (split TF32): operator images per (4 frequencies, direction)
-  unsigned short* htc16_img = nullptr;  // tensor-core Hadamard (FP16 pairs): the same images
+  unsigned short* htc16_img = nullptr;  // tensor-core Hadamard (FP16 pairs): the same images, [chunk][dir][td][sd]
+  std::shared_ptr<Tc16Images> htc16_shared;  // ... held from the per-device cache
   float* htc16_inv_sb = nullptr;        // ... and the inverse of each chunk's operator scale
   unsigned* d_bound = nullptr;          // ... and the per-eval bound of the spectra (FP32 bits)
   int* htc16_ctab = nullptr;            // ... and its colleague tables [tile][26][128]
@@ -261,11 +307,9 @@ struct Impl : ImplBase {
                 kt[dst + 1] = kh[src + 1];
               }
         if (sizeof(T) == 4 && E.m2l_tc && !E.m2l_tc_tf32 && m2l_tc16_supported(nf, sd_m, td_m)) {
-          std::vector<unsigned short> im;
-          std::vector<float> isb;
-          m2l_tc16_images(nf, op.m2l.data(), &im, &isb);
-          htc16_img = upload(im);
-          htc16_inv_sb = upload(isb);
+          htc16_shared = tc16_images(E.ops, E.device, nf, sd_m, td_m);
+          htc16_img = htc16_shared->img;
+          htc16_inv_sb = htc16_shared->inv_sb;
         } else if (sizeof(T) == 4 && E.m2l_tc && m2l_tc_supported(nf, sd_m, td_m)) {
           std::vector<float> im;
           m2l_tc_images(nf, op.m2l.data(), &im);
@@ -383,7 +427,9 @@ struct Impl : ImplBase {
       // 8 blocks from index nn on stand for an absent colleague (parent-pair form)
       // (tensor-core form: sibling-group major, node n in group (n + 7) / 8,
       // the zero block a group of its own: (nn + 15) / 8 groups of 8 nodes)
-      S_spec = std::max((size_t)(nn + 8) * sd_m, htc() ? (size_t)(nn + 15) / 8 * 8 : 0) * op.nfc * 2;
+      // (FP16 form, several source dofs: one such plane per dof)
+      S_spec = std::max((size_t)(nn + 8) * sd_m, htc() ? (size_t)(nn + 15) / 8 * 8 * (htc16_img ? sd_m : 1) : 0) *
+               op.nfc * 2;
       counters_v = (double)idx.size();
       if (ktiles || ttiles || htc()) build_pairs(work);
       counters_fwd = (double)fwdn.size();
@@ -455,6 +501,7 @@ struct Impl : ImplBase {
     geom.rootlvl = E.rootlvl;
     geom.sg = htc16_img ? 2 : htc_img ? 1 : 0;
     geom.effval_sg = htc16_img ? 1 : 0;
+    geom.plane = htc16_img ? (size_t)((nn + 15) / 8 * 8) * op.nfc : 0;
     geom.bound = d_bound;
     scl.sd = sd_m;
     for (int s = 0; s < sd_m && s < 4; s++) scl.deg[s] = op.deg[s];
@@ -619,7 +666,8 @@ struct Impl : ImplBase {
       }
       // executed MMA work: per (tile, direction, 4 frequencies) 8 MMAs of
       // 128 x 32 x 8 and 8 of 128 x 16 x 8
-      counters_tc_had = steps * (op.nfc / 4) * (8.0 * 2 * 128 * 32 * 8 + 8.0 * 2 * 128 * 16 * 8);
+      counters_tc_had = steps * (op.nfc / 4) * (8.0 * 2 * 128 * 32 * 8 + 8.0 * 2 * 128 * 16 * 8) *
+                        (htc16_img ? sd_m * td_m : 1);
       htc_dirs = upload(dirs);
       if (htc16_img) {
         std::vector<int> ct;
@@ -765,16 +813,17 @@ struct Impl : ImplBase {
     if constexpr (sizeof(T) == 4) {
       if (htc16_img) {  // the largest value a spectrum can hold, for the FP16 scale
         g.bound = d_bound + r;
-        launch_spectra_bound(sup, fwd.work, fwd.n, d_depth, E.rootlvl, op.deg[0], nsurf, d_bound + r, num_sms, st);
+        launch_spectra_bound(sup, fwd.work, fwd.n, d_depth, E.rootlvl, op.deg.data(), sd_m, nsurf, d_bound + r,
+                             num_sms, st);
         nlaunch++;
       }
     }
     launch_m2l_forward<T>(g, sup, fwd.work, fwd.n, d_depth, spec, st);
     if (prof) KCHECK(cudaEventRecord(ev[7], st));
     if (pairs_n > 0 && htc16_img) {
-      launch_m2l_hadamard_tc16(E.had_groups, op.nfc, htc16_img, reinterpret_cast<const unsigned*>(spec), pairs_n,
-                               pairs_chd, htc16_ctab, htc_dirs, reinterpret_cast<float*>(eff), d_bound + r,
-                               htc16_inv_sb, E.wait_limit, d_status, num_sms, st);
+      launch_m2l_hadamard_tc16(E.had_groups, op.nfc, sd_m, td_m, htc16_img, reinterpret_cast<const unsigned*>(spec),
+                               pairs_n, pairs_chd, htc16_ctab, htc_dirs, reinterpret_cast<float*>(eff), geom.plane,
+                               d_bound + r, htc16_inv_sb, E.wait_limit, d_status, num_sms, st);
       KCHECK(cudaGetLastError());
     } else if (pairs_n > 0 && htc_img) {
       launch_m2l_hadamard_tc(op.nfc, htc_img, reinterpret_cast<const float*>(spec), pairs_n, pairs_chd, pairs_coll,
@@ -805,7 +854,7 @@ struct Impl : ImplBase {
     nlaunch = 0;
     const int md = tr.maxdepth;
     const int K1 = nsurf * sd_m;
-    const int chunk = std::max(1, std::min(nrhs, cap_chunk));
+    const int chunk = std::max(1, std::min({nrhs, cap_chunk, E.rhs_chunk > 0 ? E.rhs_chunk : cap_chunk}));
     const bool prof = E.profiling && nrhs <= chunk;  // phase events for a single chunk
     if (prof) KCHECK(cudaEventRecord(ev[0], st));
     launch_scatter_den<T>(d_srcden, d_sperm, E.ns, sd_u, nrhs, sden, st);
@@ -907,6 +956,8 @@ struct Impl : ImplBase {
     for (int i = 0; i < 9; i++) ms[i] = pt[i];
   }
   int launches() const override { return nlaunch; }
+  int max_rhs_chunk() const override { return max_chunk; }
+  bool tunable_groups() const override { return htc16_img != nullptr && pairs_n > 0; }
 };
 
 // ---------------------------------------------------------------------------
@@ -1008,6 +1059,26 @@ int Engine::setup() {
       return KIFMM_ERR_OPTION;
     }
     had_groups = hg;
+    had_groups_set = found;
+    int rc = 0;
+    if (!parse_int(opts, "-" + prefix + "rhs_chunk", &rc, &found) || rc < 0 || rc > 8) {
+      err = "rhs_chunk must be in [0, 8]";
+      return KIFMM_ERR_OPTION;
+    }
+    rhs_chunk = rc;
+    rhs_chunk_set = found;
+    int at = 0;
+    if (!parse_int(opts, "-" + prefix + "autotune", &at, &found) || at < 0 || at > 1) {
+      err = "autotune must be 0 or 1";
+      return KIFMM_ERR_OPTION;
+    }
+    autotune = at;
+    int ar = 1;
+    if (!parse_int(opts, "-" + prefix + "autotune_rhs", &ar, &found) || ar < 1 || ar > 64) {
+      err = "autotune_rhs must be in [1, 64]";
+      return KIFMM_ERR_OPTION;
+    }
+    autotune_rhs = ar;
     if (fit != opts.end()) {
       std::string v = fit->second;
       v.erase(0, v.find_first_not_of(" \t"));
@@ -1108,7 +1179,145 @@ int Engine::setup() {
     return e.e == cudaErrorMemoryAllocation ? KIFMM_ERR_ALLOC : KIFMM_ERR_CUDA;
   }
   setup_ms[2] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t2).count();
+  setup_ms[3] = 0;
   ready = true;
+  schedule[0] = had_groups;
+  schedule[1] = rhs_chunk;
+  for (int i = 2; i < 6; i++) schedule[i] = 0;
+  if (autotune) {
+    const int rc = autotune_run();
+    if (rc != KIFMM_OK) {
+      ready = false;
+      return rc;
+    }
+  }
+  return KIFMM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Setup-time autotuner: the schedule knobs that change no result bit of
+// meaning (the FP16 Hadamard's producer groups, and how many density vectors
+// one pass of the surface contractions carries) are timed on the engine
+// itself, on autotune_rhs synthetic density vectors, one warm-up and two
+// timed evals per candidate (CUDA events on the engine stream, the faster of
+// the two), and the fastest is kept.  Choices are cached process-wide per
+// (kernel, equivalent kernel, np, precision, V-list form, size class of the
+// tree = round(2 log2 nodes), vectors), so instances of one batch that share
+// these tune once.  A knob given explicitly as an option is not tuned.
+namespace {
+struct TuneKey {
+  int kt, kt_mm, np, mixed, form, size_class, nrhs;
+  bool operator<(const TuneKey& o) const {
+    return std::tie(kt, kt_mm, np, mixed, form, size_class, nrhs) <
+           std::tie(o.kt, o.kt_mm, o.np, o.mixed, o.form, o.size_class, o.nrhs);
+  }
+};
+struct TuneVal {
+  int groups, chunk, ncand;
+  double ms;
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, TuneVal> g_tuned;
+}  // namespace
+
+int Engine::autotune_run() {
+  const auto t0 = std::chrono::steady_clock::now();
+  const int R = autotune_rhs;
+  const int form = m2l_tc ? (m2l_tc_tf32 ? 3 : 2) : (m2l_toeplitz ? 1 : 0);
+  const TuneKey key{user.kt, mm.kt, np, mixed ? 1 : 0, form,
+                    (int)std::lround(2.0 * std::log2((double)std::max(2, tree.nnodes))), R};
+  auto finish = [&](const TuneVal& v, bool cached) {
+    if (!had_groups_set) had_groups = v.groups;
+    if (!rhs_chunk_set) rhs_chunk = v.chunk;
+    schedule[0] = had_groups;
+    schedule[1] = rhs_chunk;
+    schedule[2] = 1;
+    schedule[3] = cached ? 1 : 0;
+    schedule[4] = v.ncand;
+    schedule[5] = v.ms;
+    setup_ms[3] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  };
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tuned.find(key);
+    if (it != g_tuned.end()) {
+      finish(it->second, true);
+      return KIFMM_OK;
+    }
+  }
+  std::vector<int> groups = {had_groups};
+  if (!had_groups_set && impl->tunable_groups()) groups = {2, 3};
+  std::vector<int> chunks = {rhs_chunk};
+  const int cmax = std::max(1, std::min(R, impl->max_rhs_chunk()));
+  if (!rhs_chunk_set && R > 1) {
+    chunks.clear();
+    for (int c : {1, 2, 4})
+      if (c < cmax) chunks.push_back(c);
+    chunks.push_back(cmax);
+  }
+  // synthetic densities in [-1, 1): a fixed linear congruential sequence
+  const size_t nin = (size_t)ns * user.sd * R, nout = (size_t)nt * user.td * R;
+  std::vector<double> h(nin);
+  uint64_t x = 0x9E3779B97F4A7C15ull;
+  for (size_t i = 0; i < nin; i++) {
+    x = x * 6364136223846793005ull + 1442695040888963407ull;
+    h[i] = (double)(x >> 11) * (2.0 / 9007199254740992.0) - 1.0;
+  }
+  double *din = nullptr, *dout = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  TuneVal best{had_groups, rhs_chunk, 0, 1e300};
+  int rc = KIFMM_OK;
+  try {
+    if (cudaMalloc(&din, std::max<size_t>(nin, 1) * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&dout, std::max<size_t>(nout, 1) * sizeof(double)) != cudaSuccess)
+      throw CudaError{cudaErrorMemoryAllocation, "autotune buffers"};
+    KCHECK(cudaMemcpy(din, h.data(), nin * sizeof(double), cudaMemcpyHostToDevice));
+    KCHECK(cudaEventCreate(&e0));
+    KCHECK(cudaEventCreate(&e1));
+    const bool prof = profiling;
+    profiling = false;
+    for (int g : groups)
+      for (int c : chunks) {
+        had_groups = g;
+        rhs_chunk = c;
+        double tbest = 1e300;
+        for (int it = 0; it < 3; it++) {
+          KCHECK(cudaEventRecord(e0, stream));
+          int r = impl->eval(din, dout, R, stream);
+          if (r != KIFMM_OK) throw CudaError{cudaErrorUnknown, "autotune eval"};
+          KCHECK(cudaEventRecord(e1, stream));
+          KCHECK(cudaEventSynchronize(e1));
+          float ms = 0;
+          KCHECK(cudaEventElapsedTime(&ms, e0, e1));
+          if (it > 0) tbest = std::min(tbest, (double)ms);
+        }
+        best.ncand++;
+        if (tbest < best.ms) {
+          best.ms = tbest;
+          best.groups = g;
+          best.chunk = c;
+        }
+      }
+    profiling = prof;
+    if (impl->take_status()) {
+      err = "a device-side wait timed out while autotuning";
+      rc = KIFMM_ERR_CUDA;
+    }
+  } catch (const CudaError& e) {
+    err = std::string("autotune: ") + e.where + ": " + cudaGetErrorString(e.e);
+    cudaGetLastError();
+    rc = e.e == cudaErrorMemoryAllocation ? KIFMM_ERR_ALLOC : KIFMM_ERR_CUDA;
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (din) cudaFree(din);
+  if (dout) cudaFree(dout);
+  if (rc != KIFMM_OK) return rc;
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tuned[key] = best;
+  }
+  finish(best, false);
   return KIFMM_OK;
 }
 

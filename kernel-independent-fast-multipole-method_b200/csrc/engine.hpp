@@ -23,6 +23,10 @@ struct ImplBase {
   virtual int take_status() = 0;
   virtual void phase_times(double* ms) const = 0;
   virtual int launches() const = 0;
+  // the most density vectors one pass of the surface contractions may carry
+  virtual int max_rhs_chunk() const = 0;
+  // the FP16 tensor-core Hadamard runs, so its producer groups can be tuned
+  virtual bool tunable_groups() const = 0;
 };
 
 struct Engine {
@@ -46,6 +50,14 @@ struct Engine {
   int wait_limit = 1 << 22;   // polls before a device-side pipeline wait gives up (-<prefix>wait_limit;
                               // 0: every such wait gives up at once, to exercise the time-out path)
   int had_groups = 3;         // producer groups of the FP16 tensor-core Hadamard (-<prefix>had_groups)
+  int rhs_chunk = 0;          // density vectors per pass (-<prefix>rhs_chunk; 0: as many as memory allows, <= 8)
+  int autotune = 0;           // time the candidate schedules at setup and keep the fastest (-<prefix>autotune)
+  int autotune_rhs = 1;       // density vectors per eval the schedule is tuned for (-<prefix>autotune_rhs)
+  bool had_groups_set = false, rhs_chunk_set = false;  // given as options: not tuned
+  // the schedule in use: [0] Hadamard producer groups, [1] density vectors
+  // per pass, [2] autotuned, [3] taken from the process-wide cache,
+  // [4] candidates timed, [5] best ms per eval of autotune_rhs vectors
+  double schedule[6] = {3, 0, 0, 0, 0, 0};
   bool profiling = false;
   // state
   bool ready = false;       // device state built, eval allowed
@@ -58,8 +70,9 @@ struct Engine {
   cudaStream_t stream = nullptr;
   // work counters (kifmm_work_counters)
   std::vector<double> counters;
-  // setup phases (ms): tree + lists, operators, device data and work lists
-  double setup_ms[3] = {0, 0, 0};
+  // setup phases (ms): tree + lists, operators, device data and work lists,
+  // schedule autotuning
+  double setup_ms[4] = {0, 0, 0, 0};
   // host-API staging (grown on demand)
   double* d_in = nullptr;
   double* d_out = nullptr;
@@ -70,6 +83,8 @@ struct Engine {
 
   ~Engine();
   int setup();  // returns a kifmm_status
+  // times the candidate schedules on the set-up engine (autotune option)
+  int autotune_run();
   int eval_host(const double* srcden, double* trgval, int nrhs);
   int eval_device(const double* d_srcden, double* d_trgval, int nrhs, cudaStream_t st, bool sync);
   // Enqueues the evaluation passes on st without any host synchronisation

@@ -132,10 +132,13 @@ struct M2LGeom {
   // tensor-core Hadamard, in the 8 bytes (spectra_sg_index) the FP32 value
   // would take
   const unsigned* bound = nullptr;
-  // accumulated spectra (single dof) in the sibling-group-major layout of
+  // accumulated spectra in the sibling-group-major layout of
   // spectra_sg_index instead of [node][td][nfc] (written so by the FP16
   // tensor-core Hadamard)
   int effval_sg = 0;
+  // sg == 2 and effval_sg: complex slots per dof plane of the
+  // sibling-group-major spectra (dof s at s * plane + spectra_sg_index)
+  size_t plane = 0;
 };
 // complex index of (node, compact frequency c) in the sibling-group-major
 // layout of nfc frequencies (a multiple of 4)
@@ -191,16 +194,22 @@ void launch_m2l_hadamard_tc(int nf, const float* img, const float* spectra, int 
 // 1 / inv_sb[chunk] (m2l_tc16_images).  groups: producer warp groups = TMEM A
 // stages (2 or 3 groups: 4 or 6 stages).  wait_limit bounds every pipeline
 // wait (polls); a time-out sets bit 3 of *status.
+// Equivalent kernels with sd x td dofs (1 x 1, Stokes 4 x 3, Navier 3 x 3):
+// the images are [chunk][direction][td][sd]; the source spectra and the
+// accumulated spectra hold one sibling-group-major plane of `plane` complex
+// slots per dof, and a work item is (chunk, target dof, tile) whose steps
+// are (direction, source dof).
 bool m2l_tc16_supported(int nf, int sd, int td);
-void m2l_tc16_images(int nf, const std::complex<double>* m2l, std::vector<unsigned short>* img,
+void m2l_tc16_images(int nf, int sd, int td, const std::complex<double>* m2l, std::vector<unsigned short>* img,
                      std::vector<float>* inv_sb);
-// *bound = max over nodes of 2^((depth + rootlvl) deg) * sum |supeden[node]| (one dof, FP32 bits)
-void launch_spectra_bound(const float* supeden, const int* nodes, int n, const int* depth, int rootlvl, int deg,
-                          int nsurf, unsigned* bound, int num_sms, cudaStream_t st);
-void launch_m2l_hadamard_tc16(int groups, int nf, const unsigned short* img, const unsigned* spectra, int nq,
-                              const int* qchd, const int* ctab, const unsigned* tile_dirs, float* effval,
-                              const unsigned* bound, const float* inv_sb, int wait_limit, int* status, int num_sms,
-                              cudaStream_t st);
+// *bound = max over nodes and source dofs s of 2^((depth + rootlvl) deg[s]) *
+// sum_k |supeden[node][k][s]| (FP32 bits)
+void launch_spectra_bound(const float* supeden, const int* nodes, int n, const int* depth, int rootlvl,
+                          const int* deg, int sd, int nsurf, unsigned* bound, int num_sms, cudaStream_t st);
+void launch_m2l_hadamard_tc16(int groups, int nf, int sd, int td, const unsigned short* img,
+                              const unsigned* spectra, int nq, const int* qchd, const int* ctab,
+                              const unsigned* tile_dirs, float* effval, size_t plane, const unsigned* bound,
+                              const float* inv_sb, int wait_limit, int* status, int num_sms, cudaStream_t st);
 // colleague tables of the FP16 form: per tile of 128 target parents and
 // direction, the sibling group ((first child + 7) / 8) of each row's colleague
 // (the all-zero group for an absent one or a padding row), [tile][26][128]

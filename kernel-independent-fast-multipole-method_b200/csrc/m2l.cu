@@ -480,7 +480,8 @@ __global__ void __launch_bounds__(256) k_m2l_fwd_rb(M2LGeom g, const T* __restri
           }
           if constexpr (sizeof(T) == 4) {
             if (g.sg == 2) {
-              reinterpret_cast<uint2*>(spectra)[spectra_sg_index(NFC, node, c)] = f16_pairs(re, im, s16);
+              reinterpret_cast<uint2*>(spectra)[s * g.plane + spectra_sg_index(NFC, node, c)] =
+                  f16_pairs(re, im, s16);
               continue;
             }
           }
@@ -520,8 +521,9 @@ __global__ void __launch_bounds__(256) k_m2l_inv_rb(M2LGeom g, const T* __restri
     T* dst = tdncval + (size_t)node * NSURF * g.td;
     for (int t = 0; t < g.td; t++) {
       const Cpx<T>* src = reinterpret_cast<const Cpx<T>*>(effval + ((size_t)node * g.td + t) * NFC * 2);
-      // sibling-group-major accumulated spectra (single dof): value c at spectra_sg_index
-      const Cpx<T>* srcg = reinterpret_cast<const Cpx<T>*>(effval) + spectra_sg_index(NFC, node, 0);
+      // sibling-group-major accumulated spectra: value c of dof t at
+      // t * plane + spectra_sg_index
+      const Cpx<T>* srcg = reinterpret_cast<const Cpx<T>*>(effval) + t * g.plane + spectra_sg_index(NFC, node, 0);
       // z pass (inverse), lines (ky, kx): Bm[k][ky][kx] = sum_kz Y[kz][ky][kx] w^(-k kz), k < np
       for (int line = lane; line < N * NH; line += 32) {
         const int kx = line % NH, ky = line / NH;

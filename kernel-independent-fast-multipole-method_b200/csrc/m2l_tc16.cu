@@ -215,9 +215,16 @@ constexpr int H16_NBI = 9;  // room for the operator image stages (G + 2 G for G
 constexpr size_t h16_smem(int max_items) { return (size_t)H16_NBI * H16_IMG_BYTES + 4 * (size_t)max_items; }
 
 // one step forward in a CTA's step sequence (items li in grid-stride order,
-// the directions d of each item's mask dm); false past the last item
-__device__ __forceinline__ bool h16_step(int& li, int& d, int& fc, int& tile, unsigned& dm, const unsigned* dirs,
-                                         int my_items, int ntiles) {
+// the directions d of each item's mask dm, and for each direction the SD
+// source dofs sx); false past the last item
+template <int SD>
+__device__ __forceinline__ bool h16_step(int& li, int& d, int& sx, int& fc, int& tile, unsigned& dm,
+                                         const unsigned* dirs, int my_items, int ntiles) {
+  if (SD > 1 && sx + 1 < SD) {
+    sx++;
+    return true;
+  }
+  sx = 0;
   const unsigned rest = d >= 25 ? 0u : (dm >> (d + 1));
   if (rest) {
     d += __ffs(rest);
@@ -234,12 +241,13 @@ __device__ __forceinline__ bool h16_step(int& li, int& d, int& fc, int& tile, un
   return true;
 }
 
-// G steps forward: inside an item the G-th set bit of the mask above d,
-// across an item's end single steps
-template <int G>
-__device__ __forceinline__ bool h16_stepG(int& li, int& d, int& fc, int& tile, unsigned& dm, const unsigned* dirs,
-                                          int my_items, int ntiles) {
-  if (d < 25) {
+// G steps forward: inside an item (one source dof) the G-th set bit of the
+// mask above d, across an item's end single steps; single steps throughout
+// for several source dofs
+template <int G, int SD>
+__device__ __forceinline__ bool h16_stepG(int& li, int& d, int& sx, int& fc, int& tile, unsigned& dm,
+                                          const unsigned* dirs, int my_items, int ntiles) {
+  if (SD == 1 && d < 25) {
     unsigned r = dm >> (d + 1);
 #pragma unroll
     for (int k = 0; k < G - 1; k++) r &= r - 1u;
@@ -250,15 +258,15 @@ __device__ __forceinline__ bool h16_stepG(int& li, int& d, int& fc, int& tile, u
   }
   bool ok = true;
 #pragma unroll 1
-  for (int k = 0; k < G && ok; k++) ok = h16_step(li, d, fc, tile, dm, dirs, my_items, ntiles);
+  for (int k = 0; k < G && ok; k++) ok = h16_step<SD>(li, d, sx, fc, tile, dm, dirs, my_items, ntiles);
   return ok;
 }
 
-template <int NF, int H16_G>
+template <int NF, int H16_G, int SD, int TD>
 __global__ void __launch_bounds__(h16_threads(H16_G), 1)
     k_m2l_had_tc16(const unsigned char* __restrict__ img, const unsigned* __restrict__ spectra, int nq, int ntiles,
                    const int* __restrict__ qchd, const int* __restrict__ ctab, const unsigned* __restrict__ tile_dirs,
-                   float* __restrict__ effval, int nitems, const unsigned* __restrict__ bound,
+                   float* __restrict__ effval, int nitems, size_t plane, const unsigned* __restrict__ bound,
                    const float* __restrict__ inv_sb, int wait_limit, int* __restrict__ status) {
   constexpr int H16_MMA_WARP = H16_G * 4;  // first of the 4 MMA warps
   constexpr int H16_S = 2 * H16_G;         // A stages: step s uses stage s mod S
@@ -321,10 +329,11 @@ __global__ void __launch_bounds__(h16_threads(H16_G), 1)
     const unsigned abase = tmem + H16_ACOL0 + ((unsigned)(qd * 32) << 16);
     // the group's steps s = grp, grp + G, ...: item li, direction d; the
     // item's chunk fc and tile advance by grid strides
-    int li = 0, d = -1, fc = blockIdx.x / ntiles, tile = blockIdx.x - fc * ntiles;
+    // (fc counts chunk x target dof: chunk fc / TD, target dof fc % TD)
+    int li = 0, d = -1, sx = SD - 1, fc = blockIdx.x / ntiles, tile = blockIdx.x - fc * ntiles;
     unsigned dm = dirs[0];
     bool ok = true;
-    for (int k = 0; k <= grp && ok; k++) ok = h16_step(li, d, fc, tile, dm, dirs, my_items, ntiles);
+    for (int k = 0; k <= grp && ok; k++) ok = h16_step<SD>(li, d, sx, fc, tile, dm, dirs, my_items, ntiles);
     // the colleague groups of this thread's 4 rows at the group's next step,
     // loaded one group step ahead of their use
     int g0 = 0, g1 = 0, g2 = 0, g3 = 0;
@@ -342,9 +351,12 @@ __global__ void __launch_bounds__(h16_threads(H16_G), 1)
       // the step's operator images into stage s mod NB, last read by step
       // s - NB; this group's stage wait of step s - G saw the MMAs of step
       // s - G - S complete, and NB = G + S
+      // images [chunk][direction][target dof][source dof]
+      const int fch = TD == 1 ? fc : fc / TD, tdf = TD == 1 ? 0 : fc - fch * TD;
       if (qd == 0 && lane == 0)
-        bulk_load(smem_u32(imgs + (size_t)(s % H16_NB) * H16_IMG_BYTES), img + ((size_t)fc * 26 + d) * H16_IMG_BYTES,
-                  H16_IMG_BYTES, smem_u32(&bfull[s % H16_NB]));
+        bulk_load(smem_u32(imgs + (size_t)(s % H16_NB) * H16_IMG_BYTES),
+                  img + ((((size_t)fch * 26 + d) * TD + tdf) * SD + sx) * H16_IMG_BYTES, H16_IMG_BYTES,
+                  smem_u32(&bfull[s % H16_NB]));
       if (qd == 0) pend = s;
       // all of the step's loads at once: x[h][ab][e][w] = word w
       // (frequency w / 2, {hi, lo} = w % 2) of child c + 4 e of the
@@ -353,12 +365,12 @@ __global__ void __launch_bounds__(h16_threads(H16_G), 1)
 #pragma unroll
       for (int k = 0; k < 4; k++) {
         const int gk = k == 0 ? g0 : k == 1 ? g1 : k == 2 ? g2 : g3;
-        const unsigned* src = spectra + (((size_t)gk * (NF / H16_F) + fc) * 64) + 8 * c;
+        const unsigned* src = spectra + (SD == 1 ? 0 : sx * plane * 2) + (((size_t)gk * (NF / H16_F) + fch) * 64) + 8 * c;
         ld32B(src, x[k >> 1][k & 1][0]);
         ld32B(src + 32, x[k >> 1][k & 1][1]);
       }
       const int stg = s % H16_S, sb = s % H16_NB, sbp = (s / H16_NB) & 1;
-      ok = h16_stepG<H16_G>(li, d, fc, tile, dm, dirs, my_items, ntiles);
+      ok = h16_stepG<H16_G, SD>(li, d, sx, fc, tile, dm, dirs, my_items, ntiles);
       if (ok) H16_LOAD_G()  // the g's are free once the step's loads are issued
       if (s >= H16_S && !wait(&aempty[stg], ((s / H16_S) + 1) & 1)) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -403,7 +415,7 @@ __global__ void __launch_bounds__(h16_threads(H16_G), 1)
     // A_hi of frequency f: column block 2 f, A_lo block 2 f + 1
     const unsigned acol = H16_ACOL0 + 16 * f;
     for (int li = 0; li < my_items; li++) {
-      const int nst = __popc(dirs[li]);
+      const int nst = __popc(dirs[li]) * SD;
       for (int k = 0; k < nst; k++) {
         const int stg = s % H16_S;
         if (!__all_sync(0xffffffffu, ready) && !wait(&afull[stg], (s / H16_S) & 1)) {
@@ -428,7 +440,8 @@ __global__ void __launch_bounds__(h16_threads(H16_G), 1)
       if (!wait(&accfull, li & 1)) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const int i = blockIdx.x + li * gridDim.x;
-      const int fc = i / ntiles, tile = i - fc * ntiles;
+      const int ft = i / ntiles, tile = i - ft * ntiles;
+      const int fc = TD == 1 ? ft : ft / TD, tdf = TD == 1 ? 0 : ft - fc * TD;
       const int row = (warp & 3) * 32 + lane;
       const unsigned lane_off = (unsigned)((warp & 3) * 32) << 16;
       const int q = tile * H16_M + row;
@@ -454,7 +467,7 @@ __global__ void __launch_bounds__(h16_threads(H16_G), 1)
       // sibling-group-major accumulated spectra (all 8 children; the inverse
       // pass reads only the V-list targets among them)
       if (q < nq) {
-        float* dst = effval + (((size_t)((qchd[q] + 7) >> 3) * (NF / H16_F) + fc) * 64);
+        float* dst = effval + (TD == 1 ? 0 : tdf * plane * 2) + (((size_t)((qchd[q] + 7) >> 3) * (NF / H16_F) + fc) * 64);
 #pragma unroll
         for (int ch = 0; ch < 8; ch++)
           st32B(dst + 8 * ch, y[0][2 * ch], y[0][2 * ch + 1], y[1][2 * ch], y[1][2 * ch + 1], y[2][2 * ch],
@@ -476,21 +489,25 @@ __global__ void __launch_bounds__(h16_threads(H16_G), 1)
   }
 }
 
-// bound = max over the nodes of 2^(lvl deg) * sum |supeden[node]| (one dof),
-// as FP32 bits (non-negative floats order like their bit patterns)
+// bound = max over the nodes and source dofs s of 2^(lvl deg[s]) * sum_k
+// |supeden[node][k][s]|, as FP32 bits (non-negative floats order like their
+// bit patterns)
 __global__ void __launch_bounds__(256) k_spectra_bound(const float* __restrict__ supeden, const int* __restrict__ nodes,
-                                                       int n, const int* __restrict__ depth, int rootlvl, int deg,
-                                                       int nsurf, unsigned* __restrict__ bound) {
+                                                       int n, const int* __restrict__ depth, int rootlvl, int4 deg,
+                                                       int sd, int nsurf, unsigned* __restrict__ bound) {
   float best = 0.f;
   const int lane = threadIdx.x & 31;
   for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < n; w += (gridDim.x * blockDim.x) >> 5) {
     const int node = nodes[w];
-    const float* u = supeden + (size_t)node * nsurf;
-    float s = 0.f;
-    for (int k = lane; k < nsurf; k += 32) s += fabsf(u[k]);
+    const float* u = supeden + (size_t)node * nsurf * sd;
+    for (int sx = 0; sx < sd; sx++) {
+      float s = 0.f;
+      for (int k = lane; k < nsurf; k += 32) s += fabsf(u[(size_t)k * sd + sx]);
 #pragma unroll
-    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    best = fmaxf(best, ldexpf(s, (depth[node] + rootlvl) * deg));
+      for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      const int dg = sx == 0 ? deg.x : sx == 1 ? deg.y : sx == 2 ? deg.z : deg.w;
+      best = fmaxf(best, ldexpf(s, (depth[node] + rootlvl) * dg));
+    }
   }
 #pragma unroll
   for (int o = 16; o; o >>= 1) best = fmaxf(best, __shfl_xor_sync(0xffffffffu, best, o));
@@ -505,50 +522,67 @@ __global__ void __launch_bounds__(256) k_spectra_bound(const float* __restrict__
   }
 }
 
-template <int NF, int G>
+template <int NF, int G, int SD, int TD>
 void had_tc16_launch_g(const unsigned char* img, const unsigned* spectra, int nq, const int* qchd, const int* ctab,
-                       const unsigned* tile_dirs, float* effval, const unsigned* bound, const float* inv_sb,
-                       int wait_limit, int* status, int num_sms, cudaStream_t st) {
+                       const unsigned* tile_dirs, float* effval, size_t plane, const unsigned* bound,
+                       const float* inv_sb, int wait_limit, int* status, int num_sms, cudaStream_t st) {
   const int ntiles = (nq + H16_M - 1) / H16_M;
-  const int nitems = ntiles * (NF / H16_F);
+  const int nitems = ntiles * (NF / H16_F) * TD;
   if (nitems == 0) return;
   const int grid = std::min(num_sms, nitems);
   const size_t smem = h16_smem((nitems + grid - 1) / grid);
-  auto kern = k_m2l_had_tc16<NF, G>;
+  auto kern = k_m2l_had_tc16<NF, G, SD, TD>;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  kern<<<grid, h16_threads(G), smem, st>>>(img, spectra, nq, ntiles, qchd, ctab, tile_dirs, effval, nitems, bound,
-                                           inv_sb, wait_limit, status);
+  kern<<<grid, h16_threads(G), smem, st>>>(img, spectra, nq, ntiles, qchd, ctab, tile_dirs, effval, nitems, plane,
+                                           bound, inv_sb, wait_limit, status);
+}
+
+template <int NF, int SD, int TD>
+void had_tc16_launch(int groups, const unsigned char* img, const unsigned* spectra, int nq, const int* qchd,
+                     const int* ctab, const unsigned* tile_dirs, float* effval, size_t plane, const unsigned* bound,
+                     const float* inv_sb, int wait_limit, int* status, int num_sms, cudaStream_t st) {
+  if (groups == 2)
+    had_tc16_launch_g<NF, 2, SD, TD>(img, spectra, nq, qchd, ctab, tile_dirs, effval, plane, bound, inv_sb,
+                                     wait_limit, status, num_sms, st);
+  else
+    had_tc16_launch_g<NF, 3, SD, TD>(img, spectra, nq, qchd, ctab, tile_dirs, effval, plane, bound, inv_sb,
+                                     wait_limit, status, num_sms, st);
 }
 
 template <int NF>
-void had_tc16_launch(int groups, const unsigned char* img, const unsigned* spectra, int nq, const int* qchd,
-                     const int* ctab, const unsigned* tile_dirs, float* effval, const unsigned* bound,
-                     const float* inv_sb, int wait_limit, int* status, int num_sms, cudaStream_t st) {
-  if (groups == 2)
-    had_tc16_launch_g<NF, 2>(img, spectra, nq, qchd, ctab, tile_dirs, effval, bound, inv_sb, wait_limit, status,
-                             num_sms, st);
-  else
-    had_tc16_launch_g<NF, 3>(img, spectra, nq, qchd, ctab, tile_dirs, effval, bound, inv_sb, wait_limit, status,
-                             num_sms, st);
+void had_tc16_dofs(int groups, int sd, int td, const unsigned char* img, const unsigned* spectra, int nq,
+                   const int* qchd, const int* ctab, const unsigned* tile_dirs, float* effval, size_t plane,
+                   const unsigned* bound, const float* inv_sb, int wait_limit, int* status, int num_sms,
+                   cudaStream_t st) {
+  if (sd == 1 && td == 1)
+    had_tc16_launch<NF, 1, 1>(groups, img, spectra, nq, qchd, ctab, tile_dirs, effval, plane, bound, inv_sb,
+                              wait_limit, status, num_sms, st);
+  else if (sd == 4 && td == 3)
+    had_tc16_launch<NF, 4, 3>(groups, img, spectra, nq, qchd, ctab, tile_dirs, effval, plane, bound, inv_sb,
+                              wait_limit, status, num_sms, st);
+  else if (sd == 3 && td == 3)
+    had_tc16_launch<NF, 3, 3>(groups, img, spectra, nq, qchd, ctab, tile_dirs, effval, plane, bound, inv_sb,
+                              wait_limit, status, num_sms, st);
 }
 
 }  // namespace
 
 bool m2l_tc16_supported(int nf, int sd, int td) {
-  return sd == 1 && td == 1 && (nf == 260 || nf == 868 || nf == 2052);
+  const bool dofs = (sd == 1 && td == 1) || (sd == 4 && td == 3) || (sd == 3 && td == 3);
+  return dofs && (nf == 260 || nf == 868 || nf == 2052);
 }
 
-void m2l_tc16_images(int nf, const std::complex<double>* m2l, std::vector<unsigned short>* img,
+void m2l_tc16_images(int nf, int sd, int td, const std::complex<double>* m2l, std::vector<unsigned short>* img,
                      std::vector<float>* inv_sb) {
-  const int nch = nf / H16_F;
-  img->assign((size_t)nch * 26 * (H16_IMG_BYTES / 2), 0);
+  const int nch = nf / H16_F, nts = sd * td;
+  img->assign((size_t)nch * 26 * nts * (H16_IMG_BYTES / 2), 0);
   inv_sb->assign(nch, 1.f);
   for (int fc = 0; fc < nch; fc++) {
-    // the chunk's scale: 2^(14 - e) with every |entry| <= 2^e
+    // the chunk's scale (all dof pairs): 2^(14 - e) with every |entry| <= 2^e
     double mx = 0;
-    for (int o = 0; o < 343; o++)
+    for (size_t o = 0; o < (size_t)343 * nts; o++)
       for (int f = fc * H16_F; f < fc * H16_F + H16_F; f++) {
-        const std::complex<double> t = m2l[(size_t)o * nf + f];
+        const std::complex<double> t = m2l[o * nf + f];
         mx = std::max(mx, std::max(std::abs(t.real()), std::abs(t.imag())));
       }
     int e = 0;
@@ -564,11 +598,12 @@ void m2l_tc16_images(int nf, const std::complex<double>* m2l, std::vector<unsign
                             2 * dv[2] + (j & 1) - (i & 1)};
           if (std::max(std::abs(o[0]), std::max(std::abs(o[1]), std::abs(o[2]))) <= 1) continue;  // adjacent
           const int oi = (o[0] + 3) * 49 + (o[1] + 3) * 7 + (o[2] + 3);
-          for (int fl = 0; fl < H16_F; fl++) {
-            const std::complex<double> t = m2l[(size_t)oi * nf + fc * H16_F + fl] * sb;
+          for (int ts = 0; ts < nts; ts++)  // operator [343][td][sd][nf], image [chunk][dir][td][sd]
+            for (int fl = 0; fl < H16_F; fl++) {
+            const std::complex<double> t = m2l[((size_t)oi * nts + ts) * nf + fc * H16_F + fl] * sb;
             // rows 2i + (re, im), columns 2j + (re, im): [[re, -im], [im, re]]
             const double b[2][2] = {{t.real(), -t.imag()}, {t.imag(), t.real()}};
-            unsigned short* blk = img->data() + ((size_t)fc * 26 + dir) * (H16_IMG_BYTES / 2) + fl * 512;
+            unsigned short* blk = img->data() + (((size_t)fc * 26 + dir) * nts + ts) * (H16_IMG_BYTES / 2) + fl * 512;
             for (int a = 0; a < 2; a++)
               for (int cc = 0; cc < 2; cc++) {
                 // K order of the A rows: column 2 c + e of a block = child c + 4 e
@@ -587,28 +622,29 @@ void m2l_tc16_images(int nf, const std::complex<double>* m2l, std::vector<unsign
   }
 }
 
-void launch_spectra_bound(const float* supeden, const int* nodes, int n, const int* depth, int rootlvl, int deg,
-                          int nsurf, unsigned* bound, int num_sms, cudaStream_t st) {
+void launch_spectra_bound(const float* supeden, const int* nodes, int n, const int* depth, int rootlvl,
+                          const int* deg, int sd, int nsurf, unsigned* bound, int num_sms, cudaStream_t st) {
   cudaMemsetAsync(bound, 0, sizeof(unsigned), st);
   if (n <= 0) return;
   const int grid = std::max(1, std::min(num_sms * 4, (n + 7) / 8));
-  k_spectra_bound<<<grid, 256, 0, st>>>(supeden, nodes, n, depth, rootlvl, deg, nsurf, bound);
+  const int4 dg = make_int4(deg[0], sd > 1 ? deg[1] : 0, sd > 2 ? deg[2] : 0, sd > 3 ? deg[3] : 0);
+  k_spectra_bound<<<grid, 256, 0, st>>>(supeden, nodes, n, depth, rootlvl, dg, sd, nsurf, bound);
 }
 
-void launch_m2l_hadamard_tc16(int groups, int nf, const unsigned short* img, const unsigned* spectra, int nq,
-                              const int* qchd, const int* ctab, const unsigned* tile_dirs, float* effval,
-                              const unsigned* bound, const float* inv_sb, int wait_limit, int* status, int num_sms,
-                              cudaStream_t st) {
+void launch_m2l_hadamard_tc16(int groups, int nf, int sd, int td, const unsigned short* img,
+                              const unsigned* spectra, int nq, const int* qchd, const int* ctab,
+                              const unsigned* tile_dirs, float* effval, size_t plane, const unsigned* bound,
+                              const float* inv_sb, int wait_limit, int* status, int num_sms, cudaStream_t st) {
   const unsigned char* im = reinterpret_cast<const unsigned char*>(img);
   if (nf == 868)
-    had_tc16_launch<868>(groups, im, spectra, nq, qchd, ctab, tile_dirs, effval, bound, inv_sb, wait_limit, status,
-                         num_sms, st);
+    had_tc16_dofs<868>(groups, sd, td, im, spectra, nq, qchd, ctab, tile_dirs, effval, plane, bound, inv_sb,
+                       wait_limit, status, num_sms, st);
   else if (nf == 260)
-    had_tc16_launch<260>(groups, im, spectra, nq, qchd, ctab, tile_dirs, effval, bound, inv_sb, wait_limit, status,
-                         num_sms, st);
+    had_tc16_dofs<260>(groups, sd, td, im, spectra, nq, qchd, ctab, tile_dirs, effval, plane, bound, inv_sb,
+                       wait_limit, status, num_sms, st);
   else if (nf == 2052)
-    had_tc16_launch<2052>(groups, im, spectra, nq, qchd, ctab, tile_dirs, effval, bound, inv_sb, wait_limit, status,
-                          num_sms, st);
+    had_tc16_dofs<2052>(groups, sd, td, im, spectra, nq, qchd, ctab, tile_dirs, effval, plane, bound, inv_sb,
+                        wait_limit, status, num_sms, st);
 }
 
 void m2l_tc16_tables(int nq, int zero_node, const int* coll, std::vector<int>* ctab) {

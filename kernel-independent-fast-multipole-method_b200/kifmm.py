@@ -61,6 +61,7 @@ SIGNATURES = {
     "kifmm_phase_times": [_H, _DP, _IP],
     "kifmm_set_profiling": [_H, ctypes.c_int],
     "kifmm_setup_times": [_H, _DP, _IP],
+    "kifmm_schedule": [_H, _DP, _IP],
     "kifmm_work_counters": [_H, _DP, _IP],
     "kifmm_last_launch_count": [_H, _IP],
     "kifmm_batch_create": [ctypes.c_int, ctypes.POINTER(_H), ctypes.POINTER(ctypes.c_void_p)],
@@ -273,7 +274,20 @@ class FMM3d:
         ms = (ctypes.c_double * 8)()
         n = ctypes.c_int()
         self._check(lib().kifmm_setup_times(self._h, ms, ctypes.byref(n)))
-        return dict(zip(("tree_lists", "operators", "device_build"), ms[:n.value]))
+        return dict(zip(("tree_lists", "operators", "device_build", "autotune"), ms[:n.value]))
+
+    def schedule(self):
+        """kifmm_schedule: the evaluation schedule in use (autotuned at setup
+        with -<prefix>autotune 1)."""
+        v = (ctypes.c_double * 8)()
+        n = ctypes.c_int()
+        self._check(lib().kifmm_schedule(self._h, v, ctypes.byref(n)))
+        names = ("had_groups", "rhs_chunk", "autotuned", "from_cache", "candidates", "best_ms")
+        d = {names[i]: v[i] for i in range(n.value)}
+        for k in ("had_groups", "rhs_chunk", "autotuned", "from_cache", "candidates"):
+            if k in d:
+                d[k] = int(d[k])
+        return d
 
     def work_counters(self):
         c = (ctypes.c_double * 16)()

@@ -82,6 +82,21 @@ def test_unsupported_np_and_precision():
         assert ei.value.status == kifmm.KIFMM_ERR_OPTION
 
 
+def test_engine_option_ranges():
+    # the engine's own keys: out-of-range values are option errors before any device work
+    for key, val in (("-fmm3d_had_groups", "4"), ("-fmm3d_rhs_chunk", "9"), ("-fmm3d_rhs_chunk", "-1"),
+                     ("-fmm3d_autotune", "2"), ("-fmm3d_autotune_rhs", "0"), ("-fmm3d_autotune_rhs", "65"),
+                     ("-fmm3d_wait_limit", "-1"), ("-fmm3d_m2l_form", "fft"), ("-fmm3d_tree", "gpu")):
+        o = dict(OPTS)
+        o[key] = val
+        with pytest.raises(kifmm.KifmmError) as ei:
+            make().setup(o)
+        assert ei.value.status == kifmm.KIFMM_ERR_OPTION, (key, val)
+    o = dict(OPTS, **{"-fmm3d_rhs_chunk": "4", "-fmm3d_autotune": "1", "-fmm3d_autotune_rhs": "8",
+                      "-fmm3d_had_groups": "2"})
+    setup_ok(make(), o)
+
+
 @pytest.mark.parametrize("kt", [191, 331, 391, 392, 531, 591, 592, 301, 0, -1])
 def test_kernels_rejected_by_fmm3d_setup(kt):
     # fmm3d/fmm3d_setup.cpp:53 rejects every kernel without an equivalent kernel
