@@ -165,6 +165,16 @@ struct Impl : ImplBase {
     int M = 0, K = 0;
   };
   SurfOp op_upW, op_upV, op_m2my, op_dnW, op_dnV, op_l2lz;  // factored surface operators
+  // per-level operators (E.per_level), by depth: the factors of each level and
+  // the chains from depth d to d + 1; per-level ranges of the level-ordered
+  // lists (s2m, up_all, dn_all, the V-list parents), and the sweep's operator
+  // tiles per level
+  struct LevelOps {
+    SurfOp upW, upV, m2my, dnW, dnV, l2lz;
+  };
+  std::vector<LevelOps> lv;
+  std::vector<int> off_s2m, off_up, off_dn, off_pairs;
+  std::vector<T*> ktiles_lv;
   T *ybuf, *zbuf;  // per-node rank-space coordinates of the upward / downward densities
   int ru = 0, rd = 0;  // ranks rounded up to multiples of 8 (zero-padded rows / columns)
   bool use_tc = false;
@@ -316,6 +326,9 @@ struct Impl : ImplBase {
           htc_img = upload(im);
         } else if (E.m2l_toeplitz) {
           ttiles = upload(toeplitz_tables());
+        } else if (E.per_level) {  // one set of operator tiles per level
+          for (auto& lo : E.lops->ops) ktiles_lv.push_back(upload(sweep_tiles(*lo)));
+          ktiles = ktiles_lv[0];
         } else {
           ktiles = upload(kt);
         }
@@ -396,6 +409,11 @@ struct Impl : ImplBase {
       up_all.ha = all_up_lvl;
       dn_all.hw = all_dn;
       dn_all.ha = all_dn_lvl;
+      if (E.per_level) {
+        off_s2m = level_offsets(s2m_lvl, md);
+        off_up = level_offsets(all_up_lvl, md);
+        off_dn = level_offsets(all_dn_lvl, md);
+      }
       KCHECK(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, E.device));
       gemm_ws_len = (size_t)4 << 20;  // split-K slices of the shallow levels (32 MB)
       gemm_ws = dalloc<double>(gemm_ws_len);
@@ -497,14 +515,14 @@ struct Impl : ImplBase {
     geom.surf_ijk = upload(op.surf_ijk);
     geom.sd = sd_m;
     geom.td = td_m;
-    for (int s = 0; s < sd_m && s < 4; s++) geom.deg[s] = op.deg[s];
+    for (int s = 0; s < sd_m && s < 4; s++) geom.deg[s] = E.per_level ? 0 : op.deg[s];
     geom.rootlvl = E.rootlvl;
     geom.sg = htc16_img ? 2 : htc_img ? 1 : 0;
     geom.effval_sg = htc16_img ? 1 : 0;
     geom.plane = htc16_img ? (size_t)((nn + 15) / 8 * 8) * op.nfc : 0;
     geom.bound = d_bound;
     scl.sd = sd_m;
-    for (int s = 0; s < sd_m && s < 4; s++) scl.deg[s] = op.deg[s];
+    for (int s = 0; s < sd_m && s < 4; s++) scl.deg[s] = E.per_level ? 0 : op.deg[s];
     // GEMM flops per eval
     double gf = 2.0 * ru * (nuc * td_m) * s2m.n + 2.0 * (nsurf * sd_m) * ru * up_all.n +
                 2.0 * rd * (nsurf * td_m) * dn_all.n + 2.0 * (nsurf * sd_m) * rd * dn_all.n;
@@ -519,6 +537,7 @@ struct Impl : ImplBase {
     // at most 8 (the spectra are one set, reused vector by vector)
     const double per_rhs = (double)sizeof(T) * (S_supe + S_supc + S_tdnc + S_tdne + S_y + S_z);
     max_chunk = (int)std::max(1.0, std::min(8.0, std::floor(8e9 / std::max(per_rhs, 1.0))));
+    if (E.per_level) max_chunk = 1;  // the per-level passes run on the single-vector lists
     ensure_rhs(1);
   }
 
@@ -540,7 +559,57 @@ struct Impl : ImplBase {
   // The factored operators with both ranks rounded up to multiples of 8, so
   // that every rank-space vector starts on a 32-byte boundary; the padding
   // rows and columns are zero, and so are the padded coordinates.
+  // zero-padded copy of a row-major r0 x c0 block into R x C
+  static std::vector<double> padded(const std::vector<double>& a, int r0, int c0, int R, int C) {
+    std::vector<double> o((size_t)R * C, 0.0);
+    for (int r = 0; r < r0; r++)
+      for (int c = 0; c < c0; c++) o[(size_t)r * C + c] = a[(size_t)r * c0 + c];
+    return o;
+  }
+
+  // per-level form: every level's factors and chains padded to the largest
+  // ranks over the levels
+  void build_level_ops() {
+    const LevelOperators& L = *E.lops;
+    const int nl = (int)L.ops.size();
+    int mu = 0, md_ = 0;
+    for (auto& o : L.ops) {
+      mu = std::max(mu, o->rank_up);
+      md_ = std::max(md_, o->rank_dn);
+    }
+    ru = (mu + 7) / 8 * 8;
+    rd = (md_ + 7) / 8 * 8;
+    const int K1 = nsurf * sd_m, Kuc = nuc * td_m, Kdc = nsurf * td_m;
+    use_tc = sizeof(T) == 4 && E.tensor_cores && K1 % 4 == 0 && Kuc % 4 == 0 && Kdc % 4 == 0;
+    lv.resize(nl);
+    for (int d = 0; d < nl; d++) {
+      const Operators& o = *L.ops[d];
+      lv[d].upW = make_op(padded(o.up_W, o.rank_up, Kuc, ru, Kuc), ru, Kuc);
+      lv[d].upV = make_op(padded(o.up_V, K1, o.rank_up, K1, ru), K1, ru);
+      lv[d].dnW = make_op(padded(o.dn_W, o.rank_dn, Kdc, rd, Kdc), rd, Kdc);
+      lv[d].dnV = make_op(padded(o.dn_V, K1, o.rank_dn, K1, rd), K1, rd);
+      if (d + 1 < nl) {
+        const int rc = L.ops[d + 1]->rank_up, dc = L.ops[d + 1]->rank_dn;
+        std::vector<double> m2my((size_t)ru * 8 * ru, 0.0), l2lz((size_t)8 * rd * rd, 0.0);
+        for (int r = 0; r < o.rank_up; r++)
+          for (int b = 0; b < 8; b++)
+            for (int c = 0; c < rc; c++)
+              m2my[(size_t)r * 8 * ru + (size_t)b * ru + c] = L.m2m_y[d][(size_t)r * 8 * rc + (size_t)b * rc + c];
+        for (int b = 0; b < 8; b++)
+          for (int r = 0; r < dc; r++)
+            for (int c = 0; c < o.rank_dn; c++)
+              l2lz[((size_t)b * rd + r) * rd + c] = L.l2l_z[d][((size_t)b * dc + r) * o.rank_dn + c];
+        lv[d].m2my = make_op(m2my, ru, 8 * ru);
+        lv[d].l2lz = make_op(l2lz, 8 * rd, rd);
+      }
+    }
+  }
+
   void build_surface_ops() {
+    if (E.per_level) {
+      build_level_ops();
+      return;
+    }
     const int r0u = op.rank_up, r0d = op.rank_dn;
     ru = (r0u + 7) / 8 * 8;
     rd = (r0d + 7) / 8 * 8;
@@ -570,6 +639,31 @@ struct Impl : ImplBase {
     op_dnW = make_op(dnW, rd, Kdc);
     op_dnV = make_op(dnV, K1, rd);
     op_l2lz = make_op(l2lz, 8 * rd, rd);
+  }
+
+  // operator tiles of the parent-pair sweep, [td][sd][ftile][343][32] complex
+  // (the spectra are [343][td][sd][nf])
+  std::vector<T> sweep_tiles(const Operators& o) const {
+    const int nf = o.nfc, ftiles = (nf + 31) / 32, tsd = td_m * sd_m;
+    std::vector<T> kt((size_t)tsd * ftiles * 343 * 32 * 2, T(0));
+    for (int ts = 0; ts < tsd; ts++)
+      for (int ft = 0; ft < ftiles; ft++)
+        for (int oo = 0; oo < 343; oo++)
+          for (int l = 0; l < 32 && ft * 32 + l < nf; l++) {
+            const size_t dst = ((((size_t)ts * ftiles + ft) * 343 + oo) * 32 + l) * 2;
+            const std::complex<double> v = o.m2l[((size_t)oo * tsd + ts) * nf + ft * 32 + l];
+            kt[dst] = (T)v.real();
+            kt[dst + 1] = (T)v.imag();
+          }
+    return kt;
+  }
+
+  // first index of each depth (and one past the last) in a depth-ordered list
+  static std::vector<int> level_offsets(const std::vector<int>& lvl, int md) {
+    std::vector<int> off(md + 2, 0);
+    for (int d = 0; d <= md + 1; d++)
+      off[d] = (int)(std::lower_bound(lvl.begin(), lvl.end(), d) - lvl.begin());
+    return off;
   }
 
   // Transformed operator of the Toeplitz-factored Hadamard: for direction d
@@ -631,6 +725,11 @@ struct Impl : ImplBase {
       }
     }
     std::sort(qlist.begin(), qlist.end());
+    if (E.per_level) {  // parents by depth (node ids are breadth first)
+      std::vector<int> ql;
+      for (int q : qlist) ql.push_back(tr.depth[q]);
+      off_pairs = level_offsets(ql, tr.maxdepth);
+    }
     std::vector<int> qchd, coll(qlist.size() * 26, tr.nnodes);  // absent: the zero block
     std::vector<unsigned char> mask(qlist.size(), 0);
     for (size_t w = 0; w < qlist.size(); w++) {
@@ -829,6 +928,15 @@ struct Impl : ImplBase {
       launch_m2l_hadamard_tc(op.nfc, htc_img, reinterpret_cast<const float*>(spec), pairs_n, pairs_chd, pairs_coll,
                              pairs_mask, htc_dirs, reinterpret_cast<float*>(eff), tr.nnodes, d_status, num_sms, st);
       KCHECK(cudaGetLastError());
+    } else if (pairs_n > 0 && E.per_level) {
+      // parents by depth d, their children's V lists with level d + 1's operators
+      for (int d = 0; d + 1 < (int)ktiles_lv.size(); d++) {
+        const int b = off_pairs[d], n = off_pairs[d + 1] - b;
+        if (n > 0)
+          launch_m2l_hadamard_sweep<T>(op.nfc, sd_m, td_m, ktiles_lv[d + 1], spec, n, pairs_chd + b,
+                                       pairs_coll + (size_t)b * 26, pairs_mask + b, eff, tr.nnodes, d_status, num_sms,
+                                       st);
+      }
     } else if (pairs_n > 0) {
       if (ttiles)
         launch_m2l_hadamard_tz<T>(op.nfc, sd_m, td_m, ttiles, spec, pairs_n, pairs_chd, pairs_coll, pairs_mask, eff,
@@ -869,12 +977,28 @@ struct Impl : ImplBase {
       // level and vector at once, M2M bottom-up in y coordinates, and every
       // node's density = 2^(-l deg) up_V * y
       for (int r = 0; r < R; r++) p2p(s2m, P2P_S2M, r0 + r, r, st);
-      gemm(op_upW, supcval, (int64_t)nuc * td_m, s2m.rw, ybuf, ru, s2m.rw, R * s2m.n, false, st);
-      for (int d = md - 1; d >= 2; d--) {
-        const List& P = up_non[d];
-        gemm(op_m2my, ybuf, ru, P.ra, ybuf, ru, P.rw, R * P.n, false, st);
+      if (E.per_level) {  // each level with its own operators (R = 1 here)
+        for (int d = 0; d <= md; d++) {
+          const int b = off_s2m[d];
+          gemm(lv[d].upW, supcval, (int64_t)nuc * td_m, s2m.rw + b, ybuf, ru, s2m.rw + b, off_s2m[d + 1] - b, false,
+               st);
+        }
+        for (int d = md - 1; d >= 2; d--) {
+          const List& P = up_non[d];
+          gemm(lv[d].m2my, ybuf, ru, P.ra, ybuf, ru, P.rw, P.n, false, st);
+        }
+        for (int d = 0; d <= md; d++) {
+          const int b = off_up[d];
+          gemm(lv[d].upV, ybuf, ru, up_all.rw + b, supeden, K1, up_all.rw + b, off_up[d + 1] - b, false, st);
+        }
+      } else {
+        gemm(op_upW, supcval, (int64_t)nuc * td_m, s2m.rw, ybuf, ru, s2m.rw, R * s2m.n, false, st);
+        for (int d = md - 1; d >= 2; d--) {
+          const List& P = up_non[d];
+          gemm(op_m2my, ybuf, ru, P.ra, ybuf, ru, P.rw, R * P.n, false, st);
+        }
+        gemm(op_upV, ybuf, ru, up_all.rw, supeden, K1, up_all.rw, R * up_all.n, false, st, up_all.ra);
       }
-      gemm(op_upV, ybuf, ru, up_all.rw, supeden, K1, up_all.rw, R * up_all.n, false, st, up_all.ra);
       if (prof) KCHECK(cudaEventRecord(ev[1], st));
       // V list
       KCHECK(cudaMemsetAsync(tdncval, 0, sizeof(T) * (size_t)R * S_tdnc, st));
@@ -887,12 +1011,28 @@ struct Impl : ImplBase {
       // downward: z = dn_W * check on the target nodes of every level and
       // vector at once, L2L top-down in z coordinates into the 8 children,
       // then every node's density = 2^(-l deg) dn_V * z
-      gemm(op_dnW, tdncval, (int64_t)nsurf * td_m, dn_all.rw, zbuf, rd, dn_all.rw, R * dn_all.n, false, st);
-      for (int d = 3; d <= md; d++) {
-        const List& P = dn_par[d];
-        gemm(op_l2lz, zbuf, rd, P.rw, zbuf, rd, P.ra, R * P.n, true, st);
+      if (E.per_level) {
+        for (int d = 0; d <= md; d++) {
+          const int b = off_dn[d];
+          gemm(lv[d].dnW, tdncval, (int64_t)nsurf * td_m, dn_all.rw + b, zbuf, rd, dn_all.rw + b, off_dn[d + 1] - b,
+               false, st);
+        }
+        for (int d = 3; d <= md; d++) {  // parents at depth d - 1
+          const List& P = dn_par[d];
+          gemm(lv[d - 1].l2lz, zbuf, rd, P.rw, zbuf, rd, P.ra, P.n, true, st);
+        }
+        for (int d = 0; d <= md; d++) {
+          const int b = off_dn[d];
+          gemm(lv[d].dnV, zbuf, rd, dn_all.rw + b, tdneden, K1, dn_all.rw + b, off_dn[d + 1] - b, false, st);
+        }
+      } else {
+        gemm(op_dnW, tdncval, (int64_t)nsurf * td_m, dn_all.rw, zbuf, rd, dn_all.rw, R * dn_all.n, false, st);
+        for (int d = 3; d <= md; d++) {
+          const List& P = dn_par[d];
+          gemm(op_l2lz, zbuf, rd, P.rw, zbuf, rd, P.ra, R * P.n, true, st);
+        }
+        gemm(op_dnV, zbuf, rd, dn_all.rw, tdneden, K1, dn_all.rw, R * dn_all.n, false, st, dn_all.ra);
       }
-      gemm(op_dnV, zbuf, rd, dn_all.rw, tdneden, K1, dn_all.rw, R * dn_all.n, false, st, dn_all.ra);
       if (prof) KCHECK(cudaEventRecord(ev[4], st));
       // leaves
       for (int r = 0; r < R; r++) {
@@ -1104,6 +1244,35 @@ int Engine::setup() {
     err = "kernel not supported by FMM3d";
     return KIFMM_ERR_KERNEL;
   }
+  per_level = false;
+  {
+    auto oit = opts.find("-" + prefix + "operators");
+    if (oit != opts.end()) {
+      std::string v = oit->second;
+      v.erase(0, v.find_first_not_of(" \t"));
+      v = v.substr(0, v.find_first_of(" \t%"));
+      if (v == "per_level")
+        per_level = true;
+      else if (v != "scaled") {
+        err = "operators must be scaled or per_level";
+        return KIFMM_ERR_OPTION;
+      }
+    }
+    if (per_level) {
+      // the per-level operators run with the direct parent-pair V-list form
+      auto fit = opts.find("-" + prefix + "m2l_form");
+      if (fit != opts.end() && fit->second.find("direct") == std::string::npos) {
+        err = "per_level operators use the direct V-list form (-" + prefix + "m2l_form direct)";
+        return KIFMM_ERR_OPTION;
+      }
+      if (np != 4 && np != 6 && np != 8) {
+        err = "per_level operators need np = 4, 6 or 8";
+        return KIFMM_ERR_OPTION;
+      }
+      m2l_tc = false;
+      m2l_toeplitz = false;
+    }
+  }
   bool tree_on_device = true;
   {
     auto tit = opts.find("-" + prefix + "tree");
@@ -1144,6 +1313,11 @@ int Engine::setup() {
   auto t1 = std::chrono::steady_clock::now();
   ops = get_operators(mm, np, host_threads(), &err);
   if (!ops) return KIFMM_ERR_NUMERIC;
+  lops.reset();
+  if (per_level) {
+    lops = get_level_operators(mm, np, rootlvl, rootlvl + std::max(tree.maxdepth, 0), host_threads(), &err);
+    if (!lops) return KIFMM_ERR_NUMERIC;
+  }
   auto t2 = std::chrono::steady_clock::now();
   setup_ms[0] = std::chrono::duration<double, std::milli>(t1 - t0).count();
   setup_ms[1] = std::chrono::duration<double, std::milli>(t2 - t1).count();

@@ -50,6 +50,10 @@ struct Engine {
   int wait_limit = 1 << 22;   // polls before a device-side pipeline wait gives up (-<prefix>wait_limit;
                               // 0: every such wait gives up at once, to exercise the time-out path)
   int had_groups = 3;         // producer groups of the FP16 tensor-core Hadamard (-<prefix>had_groups)
+  // -<prefix>operators per_level: the reference's non-homogeneous operator
+  // path (one operator set per level at that level's radius, no 2^(+-l deg)
+  // scaling; fmm3d/matmgnt3d.cpp:93-361 with _hom == false)
+  bool per_level = false;
   int rhs_chunk = 0;          // density vectors per pass (-<prefix>rhs_chunk; 0: as many as memory allows, <= 8)
   int autotune = 0;           // time the candidate schedules at setup and keep the fastest (-<prefix>autotune)
   int autotune_rhs = 1;       // density vectors per eval the schedule is tuned for (-<prefix>autotune_rhs)
@@ -65,6 +69,7 @@ struct Engine {
   std::string err;
   Tree tree;
   std::shared_ptr<const Operators> ops;
+  std::shared_ptr<const LevelOperators> lops;  // per_level: operators by depth (absolute level rootlvl + depth)
   std::unique_ptr<ImplBase> impl;
   int device = 0;
   cudaStream_t stream = nullptr;

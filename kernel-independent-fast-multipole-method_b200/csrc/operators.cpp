@@ -353,12 +353,21 @@ void parallel_range(int n, int nthreads, F&& f) {
   for (auto& x : th) x.join();
 }
 
-std::shared_ptr<Operators> build_operators(const KernelDesc& mm, int np, int nthreads, std::string* err) {
+// level < 0: the homogeneous form (R = 1, scaled per level by 2^(+-l deg));
+// level >= 0: the per-level form at R = 2^-level (see Operators)
+std::shared_ptr<Operators> build_operators(const KernelDesc& mm, int np, int nthreads, std::string* err,
+                                           int level = -1) {
   auto op = std::make_shared<Operators>();
   Operators& o = *op;
   o.mm = mm;
   o.np = np;
-  homogeneous_degrees(mm.kt, &o.deg);
+  o.level = level;
+  const double R = level < 0 ? 1.0 : std::ldexp(1.0, -level);
+  o.R = R;
+  if (level < 0)
+    homogeneous_degrees(mm.kt, &o.deg);
+  else
+    o.deg.assign(mm.sd, 0);
   surface_grid(np, 1.0, &o.ue, &o.surf_ijk);  // MatMgnt3d::setup, fmm3d/matmgnt3d.cpp:51-54
   surface_grid(np + 2, 3.0, &o.uc, nullptr);
   surface_grid(np, 3.0, &o.de, nullptr);
@@ -371,16 +380,23 @@ std::shared_ptr<Operators> build_operators(const KernelDesc& mm, int np, int nth
   const int sd = mm.sd, td = mm.td, ns = o.nsurf, nc = o.nuc;
   const double cut = std::pow(0.1, np + 1);  // MatMgnt3d::alt, fmm3d/matmgnt3d.cpp:38-41
 
-  // UC2UE = pinv(K(UC <- UE)) at level 0 (fmm3d/matmgnt3d.cpp:96-105)
+  // the grids at this form's radius (R = 1 in the homogeneous form)
+  auto scaled = [R](const std::vector<double>& v) {
+    std::vector<double> s(v.size());
+    for (size_t i = 0; i < v.size(); i++) s[i] = R * v[i];
+    return s;
+  };
+  const std::vector<double> ueR = scaled(o.ue), ucR = scaled(o.uc), deR = scaled(o.de), dcR = scaled(o.dc);
+  // UC2UE = pinv(K(UC <- UE)) (fmm3d/matmgnt3d.cpp:96-105)
   std::vector<double> ue2ucm((size_t)nc * td * ns * sd);
-  kernel_matrix(mm, nc, o.uc.data(), ns, o.ue.data(), o.ue.data(), ue2ucm.data());
+  kernel_matrix(mm, nc, ucR.data(), ns, ueR.data(), ueR.data(), ue2ucm.data());
   if (!pinv_factors(nc * td, ns * sd, ue2ucm.data(), cut, nthreads, &o.up_V, &o.up_W, &o.rank_up)) {
     if (err) *err = "UC2UE SVD did not converge";
     return nullptr;
   }
   // DC2DE = pinv(K(DC <- DE)) (fmm3d/matmgnt3d.cpp:163-172)
   std::vector<double> de2dcm((size_t)ns * td * ns * sd);
-  kernel_matrix(mm, ns, o.dc.data(), ns, o.de.data(), o.de.data(), de2dcm.data());
+  kernel_matrix(mm, ns, dcR.data(), ns, deR.data(), deR.data(), de2dcm.data());
   if (!pinv_factors(ns * td, ns * sd, de2dcm.data(), cut, nthreads, &o.dn_V, &o.dn_W, &o.rank_dn)) {
     if (err) *err = "DC2DE SVD did not converge";
     return nullptr;
@@ -393,26 +409,36 @@ std::shared_ptr<Operators> build_operators(const KernelDesc& mm, int np, int nth
   // scaled x0.5 and shifted by (idx-0.5) (:199-203), on z = dn_W * (check values).
   const int K1 = ns * sd;
   const int ru = o.rank_up, rd = o.rank_dn;
-  o.m2m_y.assign((size_t)ru * 8 * ru, 0.0);
-  o.l2l_z.assign((size_t)8 * rd * rd, 0.0);
+  if (level < 0) {
+    o.m2m_y.assign((size_t)ru * 8 * ru, 0.0);
+    o.l2l_z.assign((size_t)8 * rd * rd, 0.0);
+  } else {
+    o.ue2uc_raw.assign((size_t)8 * nc * td * K1, 0.0);
+    o.de2dc_raw.assign((size_t)8 * ns * td * K1, 0.0);
+  }
   parallel_range(8, nthreads, [&](int oct) {
     int idx[3] = {(oct >> 2) & 1, (oct >> 1) & 1, oct & 1};
     std::vector<double> chk(o.uc.size()), den(o.ue.size());
-    for (size_t i = 0; i < o.uc.size(); i++) chk[i] = 2.0 * o.uc[i];
+    for (size_t i = 0; i < o.uc.size(); i++) chk[i] = 2.0 * R * o.uc[i];
     for (int j = 0; j < ns; j++)
-      for (int d = 0; d < 3; d++) den[3 * j + d] = o.ue[3 * j + d] + (2 * idx[d] - 1);
+      for (int d = 0; d < 3; d++) den[3 * j + d] = R * o.ue[3 * j + d] + (2 * idx[d] - 1) * R;
     std::vector<double> ue2uc((size_t)nc * td * K1);
     kernel_matrix(mm, nc, chk.data(), ns, den.data(), den.data(), ue2uc.data());
+    std::vector<double> dchk(o.dc.size());
+    for (int j = 0; j < ns; j++)
+      for (int d = 0; d < 3; d++) dchk[3 * j + d] = 0.5 * R * o.dc[3 * j + d] + (double(idx[d]) - 0.5) * R;
+    std::vector<double> de2dc((size_t)ns * td * K1);
+    kernel_matrix(mm, ns, dchk.data(), ns, deR.data(), deR.data(), de2dc.data());
+    if (level >= 0) {  // chained with the neighbouring levels by get_level_operators
+      std::copy(ue2uc.begin(), ue2uc.end(), o.ue2uc_raw.begin() + (size_t)oct * nc * td * K1);
+      std::copy(de2dc.begin(), de2dc.end(), o.de2dc_raw.begin() + (size_t)oct * ns * td * K1);
+      return;
+    }
     std::vector<double> qb((size_t)ru * K1), qy((size_t)ru * ru);
     matmul(ru, nc * td, K1, o.up_W.data(), ue2uc.data(), qb.data());
     matmul(ru, K1, ru, qb.data(), o.up_V.data(), qy.data());
     for (int r = 0; r < ru; r++)
       for (int c = 0; c < ru; c++) o.m2m_y[(size_t)r * 8 * ru + (size_t)oct * ru + c] = qy[(size_t)r * ru + c];
-    std::vector<double> dchk(o.dc.size());
-    for (int j = 0; j < ns; j++)
-      for (int d = 0; d < 3; d++) dchk[3 * j + d] = 0.5 * o.dc[3 * j + d] + (double(idx[d]) - 0.5);
-    std::vector<double> de2dc((size_t)ns * td * K1);
-    kernel_matrix(mm, ns, dchk.data(), ns, o.de.data(), o.de.data(), de2dc.data());
     std::vector<double> rb((size_t)rd * K1), rz((size_t)rd * rd);
     matmul(rd, ns * td, K1, o.dn_W.data(), de2dc.data(), rb.data());
     matmul(rd, K1, rd, rb.data(), o.dn_V.data(), rz.data());
@@ -467,8 +493,9 @@ std::shared_ptr<Operators> build_operators(const KernelDesc& mm, int np, int nth
     for (int gz = 0; gz < n; gz++)
       for (int gy = 0; gy < n; gy++)
         for (int gx = 0; gx < n; gx++) {
-          double x[3] = {(gx < np ? gx : gx - n) * step - 2.0 * dx, (gy < np ? gy : gy - n) * step - 2.0 * dy,
-                         (gz < np ? gz : gz - n) * step - 2.0 * dz};
+          // (at R = 2^-level in the per-level form, fmm3d/matmgnt3d.cpp:308-309)
+          double x[3] = {R * ((gx < np ? gx : gx - n) * step - 2.0 * dx), R * ((gy < np ? gy : gy - n) * step - 2.0 * dy),
+                         R * ((gz < np ? gz : gz - n) * step - 2.0 * dz)};
           block(mm, x, x, b);
           size_t g = ((size_t)gz * n + gy) * n + gx;
           for (int e = 0; e < td * sd; e++) kg[g * td * sd + e] = b[e];
@@ -506,17 +533,60 @@ std::shared_ptr<Operators> build_operators(const KernelDesc& mm, int np, int nth
 
 }  // namespace
 
-std::shared_ptr<const Operators> get_operators(const KernelDesc& mm, int np, int nthreads, std::string* err) {
+namespace {
+std::shared_ptr<const Operators> cached_operators(const KernelDesc& mm, int np, int level, int nthreads,
+                                                  std::string* err) {
   static std::mutex mu;
-  static std::map<std::tuple<int, double, double, int>, std::shared_ptr<const Operators>> cache;
+  static std::map<std::tuple<int, double, double, int, int>, std::shared_ptr<const Operators>> cache;
   std::lock_guard<std::mutex> lock(mu);
-  auto key = std::make_tuple(mm.kt, mm.coefs[0], mm.coefs[1], np);
+  auto key = std::make_tuple(mm.kt, mm.coefs[0], mm.coefs[1], np, level);
   auto it = cache.find(key);
   if (it != cache.end()) return it->second;
-  auto op = build_operators(mm, np, nthreads, err);
+  auto op = build_operators(mm, np, nthreads, err, level);
   if (!op) return nullptr;
   cache[key] = op;
   return op;
+}
+}  // namespace
+
+std::shared_ptr<const Operators> get_operators(const KernelDesc& mm, int np, int nthreads, std::string* err) {
+  return cached_operators(mm, np, -1, nthreads, err);
+}
+
+std::shared_ptr<const LevelOperators> get_level_operators(const KernelDesc& mm, int np, int lmin, int lmax,
+                                                          int nthreads, std::string* err) {
+  auto L = std::make_shared<LevelOperators>();
+  L->lmin = lmin;
+  L->lmax = lmax;
+  for (int l = lmin; l <= lmax; l++) {
+    auto o = cached_operators(mm, np, l, nthreads, err);
+    if (!o) return nullptr;
+    L->ops.push_back(o);
+  }
+  const int nl = lmax - lmin + 1;
+  L->m2m_y.resize(nl);
+  L->l2l_z.resize(nl);
+  for (int i = 0; i + 1 < nl; i++) {
+    const Operators& p = *L->ops[i];      // parent level
+    const Operators& c = *L->ops[i + 1];  // child level
+    const int K1 = p.nsurf * mm.sd, Kuc = p.nuc * mm.td, Kdc = p.nsurf * mm.td;
+    const int rp = p.rank_up, rc = c.rank_up, dp = p.rank_dn, dc = c.rank_dn;
+    L->m2m_y[i].assign((size_t)rp * 8 * rc, 0.0);
+    L->l2l_z[i].assign((size_t)8 * dc * dp, 0.0);
+    parallel_range(8, nthreads, [&](int oct) {
+      std::vector<double> qb((size_t)rp * K1), qy((size_t)rp * rc);
+      matmul(rp, Kuc, K1, p.up_W.data(), c.ue2uc_raw.data() + (size_t)oct * Kuc * K1, qb.data());
+      matmul(rp, K1, rc, qb.data(), c.up_V.data(), qy.data());
+      for (int r = 0; r < rp; r++)
+        for (int k = 0; k < rc; k++) L->m2m_y[i][(size_t)r * 8 * rc + (size_t)oct * rc + k] = qy[(size_t)r * rc + k];
+      std::vector<double> rb((size_t)dc * K1), rz((size_t)dc * dp);
+      matmul(dc, Kdc, K1, c.dn_W.data(), p.de2dc_raw.data() + (size_t)oct * Kdc * K1, rb.data());
+      matmul(dc, K1, dp, rb.data(), p.dn_V.data(), rz.data());
+      for (int r = 0; r < dc; r++)
+        for (int k = 0; k < dp; k++) L->l2l_z[i][((size_t)oct * dc + r) * dp + k] = rz[(size_t)r * dp + k];
+    });
+  }
+  return L;
 }
 
 }  // namespace kifmm

@@ -76,10 +76,36 @@ struct Operators {
   std::vector<double> dn_W;    // rank_dn x (nsurf*td)
   std::vector<double> dn_V;    // (nsurf*sd) x rank_dn
   std::vector<double> l2l_z;   // (8*rank_dn) x rank_dn: row block o = dn_W * DE2DC_o * dn_V
+  // Per-level form (the reference's non-homogeneous branch, _hom == false in
+  // fmm3d/matmgnt3d.cpp:93-361): every operator built at this level's box
+  // radius R = 2^-level instead of at R = 1, no 2^(+-l deg) scaling (deg all
+  // zero), and the two child/parent matrices kept raw so that the level set
+  // can chain them with the neighbouring level's factors:
+  //   ue2uc_raw[o]  K(2R UC <- R UE + (2 idx_o - 1) R)   children at this level
+  //   de2dc_raw[o]  K(R DC / 2 + (idx_o - 1/2) R <- R DE) parent at this level
+  int level = -1;  // < 0: the homogeneous (scaled) form at R = 1
+  double R = 1.0;
+  std::vector<double> ue2uc_raw;  // [8][(nuc*td) x (nsurf*sd)]
+  std::vector<double> de2dc_raw;  // [8][(nsurf*td) x (nsurf*sd)]
 };
 
 // Builds (or returns the cached) operators; nullptr + err on failure.
 std::shared_ptr<const Operators> get_operators(const KernelDesc& mm, int np, int nthreads, std::string* err);
+
+// The per-level operator set for absolute levels lmin..lmax: ops[l - lmin]
+// built at R = 2^-l, and the rank-space chains between neighbouring levels
+//   m2m_y[l - lmin]  (rank_up(l) x 8 rank_up(l+1)), block o =
+//                    up_W(l) * ue2uc_raw(l+1)[o] * up_V(l+1)
+//   l2l_z[l - lmin]  (8 rank_dn(l+1) x rank_dn(l)), row block o =
+//                    dn_W(l+1) * de2dc_raw(l)[o] * dn_V(l)
+// (fmm3d/matmgnt3d.cpp:125-156, 190-221 with R = 2^-l).
+struct LevelOperators {
+  int lmin = 0, lmax = 0;
+  std::vector<std::shared_ptr<const Operators>> ops;
+  std::vector<std::vector<double>> m2m_y, l2l_z;
+};
+std::shared_ptr<const LevelOperators> get_level_operators(const KernelDesc& mm, int np, int lmin, int lmax,
+                                                          int nthreads, std::string* err);
 
 // Surface grid of MatMgnt3d::splposcal(np, R): the np^3 lattice on [-R,R]^3
 // restricted to its boundary, x outermost and z innermost.

@@ -86,7 +86,8 @@ def test_engine_option_ranges():
     # the engine's own keys: out-of-range values are option errors before any device work
     for key, val in (("-fmm3d_had_groups", "4"), ("-fmm3d_rhs_chunk", "9"), ("-fmm3d_rhs_chunk", "-1"),
                      ("-fmm3d_autotune", "2"), ("-fmm3d_autotune_rhs", "0"), ("-fmm3d_autotune_rhs", "65"),
-                     ("-fmm3d_wait_limit", "-1"), ("-fmm3d_m2l_form", "fft"), ("-fmm3d_tree", "gpu")):
+                     ("-fmm3d_wait_limit", "-1"), ("-fmm3d_m2l_form", "fft"), ("-fmm3d_tree", "gpu"),
+                     ("-fmm3d_operators", "homogeneous")):
         o = dict(OPTS)
         o[key] = val
         with pytest.raises(kifmm.KifmmError) as ei:
@@ -95,6 +96,13 @@ def test_engine_option_ranges():
     o = dict(OPTS, **{"-fmm3d_rhs_chunk": "4", "-fmm3d_autotune": "1", "-fmm3d_autotune_rhs": "8",
                       "-fmm3d_had_groups": "2"})
     setup_ok(make(), o)
+    # the per-level (non-homogeneous) operators run with the direct V-list form, np 4, 6 or 8
+    for extra in ({"-fmm3d_m2l_form": "toeplitz"}, {"-fmm3d_np": "5"}):
+        o = dict(OPTS, **{"-fmm3d_operators": "per_level"}, **extra)
+        with pytest.raises(kifmm.KifmmError) as ei:
+            make().setup(o)
+        assert ei.value.status == kifmm.KIFMM_ERR_OPTION, extra
+    setup_ok(make(), dict(OPTS, **{"-fmm3d_operators": "per_level", "-fmm3d_m2l_form": "direct"}))
 
 
 @pytest.mark.parametrize("kt", [191, 331, 391, 392, 531, 591, 592, 301, 0, -1])
