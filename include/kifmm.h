@@ -73,7 +73,11 @@ kifmm_status kifmm_set_box(kifmm_handle h, const double ctr[3], int rootlvl);
  * Hadamard's form), -<prefix>tensor_cores (0|1), -<prefix>wait_limit,
  * -<prefix>had_groups (2|3), -<prefix>rhs_chunk (0..8), -<prefix>autotune
  * (0|1) and -<prefix>autotune_rhs (1..64): see kifmm_poll_status and
- * kifmm_schedule. */
+ * kifmm_schedule.  -<prefix>operators (scaled|per_level) selects the
+ * reference's homogeneous operators (built once, rescaled by 2^(+-l deg)
+ * per level) or its non-homogeneous branch (built at every level's radius,
+ * fmm3d/matmgnt3d.cpp:93-361 with _hom == false; np 4, 6 or 8, direct
+ * V-list form). */
 kifmm_status kifmm_set_option(kifmm_handle h, const char* key, const char* value);
 
 /* Replaces FMM3d::setup(map<string,string>&) (fmm3d/fmm3d_setup.cpp:26-63):

@@ -79,15 +79,23 @@ namespace kifmm {
 namespace {
 
 constexpr int H16_M = 128;                       // target parents per tile (MMA M, TMEM lanes)
-constexpr int H16_F = 4;                         // frequencies per item
-// G producer groups (2 or 3), 2 G A stages (128 + 128 G TMEM columns), MMA
-// warps from warp 4 G on, 3 G operator image stages
+// G producer groups (2 or 3), 2 G A stages, MMA warps from warp 4 G on,
+// 3 G operator image stages
 constexpr int h16_threads(int G) { return (4 * G + 4) * 32; }
-constexpr unsigned H16_IMG_BYTES = H16_F * 1024;  // per (chunk, direction): F x [32 rows x 16 K] fp16
-constexpr unsigned H16_COLS = 512;               // accumulator 0-127, A stages 128-511
-constexpr unsigned H16_ACOL0 = H16_F * 32;
-constexpr unsigned H16_ACOLS = 64;               // TMEM columns per A stage
+constexpr unsigned H16_COLS = 512;
 constexpr int H16_LONG_WAIT = 1 << 22;           // polls of the end-of-CTA waits
+// Per target-dof count TD (1, or 3 for Stokes and Navier): FI frequencies
+// per item, every target dof's accumulator resident in TMEM (TD x FI x 32
+// columns from column 0), A stages of FI x 16 columns after them, operator
+// images of TD x FI x 1 KB per step (all target dofs of one source dof and
+// direction)
+template <int TD>
+struct H16Shape {
+  static constexpr int FI = TD == 1 ? 4 : 2;
+  static constexpr unsigned ACOL0 = TD * FI * 32;
+  static constexpr unsigned ACOLS = FI * 16;
+  static constexpr unsigned IMGB = TD * FI * 1024;
+};
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 
@@ -185,6 +193,11 @@ __device__ __forceinline__ void ld32B(const unsigned* p, unsigned* r) {
                : "l"(p));
 }
 
+// one 16-byte read-only load
+__device__ __forceinline__ void ld16B(const unsigned* p, unsigned* r) {
+  asm volatile("ld.global.nc.v4.b32 {%0,%1,%2,%3}, [%4];" : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "l"(p));
+}
+
 // one 32-byte store
 __device__ __forceinline__ void st32B(float* p, float a, float b, float c, float d, float e, float f, float g, float h) {
   asm volatile("st.global.v8.f32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(p), "f"(a), "f"(b), "f"(c), "f"(d), "f"(e),
@@ -212,7 +225,7 @@ __device__ __forceinline__ float inv_data_scale(float b) {
 constexpr int H16_NBI = 9;  // room for the operator image stages (G + 2 G for G <= 3)
 
 // dynamic shared memory: image stages, then the CTA's item direction masks
-constexpr size_t h16_smem(int max_items) { return (size_t)H16_NBI * H16_IMG_BYTES + 4 * (size_t)max_items; }
+constexpr size_t h16_smem(unsigned imgb, int max_items) { return (size_t)H16_NBI * imgb + 4 * (size_t)max_items; }
 
 // one step forward in a CTA's step sequence (items li in grid-stride order,
 // the directions d of each item's mask dm, and for each direction the SD
@@ -271,11 +284,13 @@ __global__ void __launch_bounds__(h16_threads(H16_G), 1)
   constexpr int H16_MMA_WARP = H16_G * 4;  // first of the 4 MMA warps
   constexpr int H16_S = 2 * H16_G;         // A stages: step s uses stage s mod S
   constexpr int H16_NB = H16_G + H16_S;    // operator image stages: step s uses s mod NB
-  static_assert(H16_ACOL0 + H16_S * H16_ACOLS <= H16_COLS, "A stages fit in TMEM");
+  constexpr int FI = H16Shape<TD>::FI;
+  constexpr unsigned ACOL0 = H16Shape<TD>::ACOL0, ACOLS = H16Shape<TD>::ACOLS, IMGB = H16Shape<TD>::IMGB;
+  static_assert(ACOL0 + H16_S * ACOLS <= H16_COLS, "A stages fit in TMEM");
   static_assert(H16_NB <= H16_NBI, "image stages");
   extern __shared__ __align__(1024) unsigned char smem[];
-  unsigned char* imgs = smem;                                       // [NB][4 KB]
-  unsigned* dirs = reinterpret_cast<unsigned*>(smem + (size_t)H16_NBI * H16_IMG_BYTES);
+  unsigned char* imgs = smem;                                       // [NB][IMGB]
+  unsigned* dirs = reinterpret_cast<unsigned*>(smem + (size_t)H16_NBI * IMGB);
   __shared__ __align__(8) unsigned long long afull[H16_S], aempty[H16_S], bfull[H16_NB], accfull, accempty, lastbar;
   __shared__ unsigned tmem_base;
   __shared__ int fail;
@@ -296,12 +311,12 @@ __global__ void __launch_bounds__(h16_threads(H16_G), 1)
   if (tid == 0) {
     for (int b = 0; b < H16_S; b++) {
       mbar_init(smem_u32(&afull[b]), 128);
-      mbar_init(smem_u32(&aempty[b]), H16_F);
+      mbar_init(smem_u32(&aempty[b]), 4);
     }
     for (int b = 0; b < H16_NB; b++) mbar_init(smem_u32(&bfull[b]), 1);
-    mbar_init(smem_u32(&accfull), H16_F);
+    mbar_init(smem_u32(&accfull), 4);
     mbar_init(smem_u32(&accempty), 128);
-    mbar_init(smem_u32(&lastbar), H16_F);
+    mbar_init(smem_u32(&lastbar), 4);
     fail = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -326,10 +341,10 @@ __global__ void __launch_bounds__(h16_threads(H16_G), 1)
     // of each half and children c, c + 4 (c = t % 4) of each row's colleague
     const int grp = warp >> 2, qd = warp & 3, c = lane & 3;
     const int rbase = qd * 32 + (lane >> 2);
-    const unsigned abase = tmem + H16_ACOL0 + ((unsigned)(qd * 32) << 16);
-    // the group's steps s = grp, grp + G, ...: item li, direction d; the
-    // item's chunk fc and tile advance by grid strides
-    // (fc counts chunk x target dof: chunk fc / TD, target dof fc % TD)
+    const unsigned abase = tmem + ACOL0 + ((unsigned)(qd * 32) << 16);
+    // the group's steps s = grp, grp + G, ...: item li, direction d, source
+    // dof sx; the item's chunk fc (of FI frequencies) and tile advance by
+    // grid strides
     int li = 0, d = -1, sx = SD - 1, fc = blockIdx.x / ntiles, tile = blockIdx.x - fc * ntiles;
     unsigned dm = dirs[0];
     bool ok = true;
@@ -351,23 +366,30 @@ __global__ void __launch_bounds__(h16_threads(H16_G), 1)
       // the step's operator images into stage s mod NB, last read by step
       // s - NB; this group's stage wait of step s - G saw the MMAs of step
       // s - G - S complete, and NB = G + S
-      // images [chunk][direction][target dof][source dof]
-      const int fch = TD == 1 ? fc : fc / TD, tdf = TD == 1 ? 0 : fc - fch * TD;
+      // images [chunk][direction][source dof][target dof][frequency]
       if (qd == 0 && lane == 0)
-        bulk_load(smem_u32(imgs + (size_t)(s % H16_NB) * H16_IMG_BYTES),
-                  img + ((((size_t)fch * 26 + d) * TD + tdf) * SD + sx) * H16_IMG_BYTES, H16_IMG_BYTES,
+        bulk_load(smem_u32(imgs + (size_t)(s % H16_NB) * IMGB), img + (((size_t)fc * 26 + d) * SD + sx) * IMGB, IMGB,
                   smem_u32(&bfull[s % H16_NB]));
       if (qd == 0) pend = s;
       // all of the step's loads at once: x[h][ab][e][w] = word w
-      // (frequency w / 2, {hi, lo} = w % 2) of child c + 4 e of the
-      // colleague of row (h, ab), so the step waits for memory once
-      unsigned x[2][2][2][8];
+      // (frequency w / 2 of the chunk, {hi, lo} = w % 2) of child c + 4 e of
+      // the colleague of row (h, ab), so the step waits for memory once; a
+      // child's 4 frequencies of a 256-byte block are 8 words, FI = 2 takes
+      // half of them
+      unsigned x[2][2][2][2 * FI];
+      const size_t sbase = (SD == 1 ? 0 : sx * plane * 2) + (size_t)(FI == 4 ? fc : fc >> 1) * 64 + 8 * c +
+                           (FI == 4 ? 0 : (fc & 1) * 4);
 #pragma unroll
       for (int k = 0; k < 4; k++) {
         const int gk = k == 0 ? g0 : k == 1 ? g1 : k == 2 ? g2 : g3;
-        const unsigned* src = spectra + (SD == 1 ? 0 : sx * plane * 2) + (((size_t)gk * (NF / H16_F) + fch) * 64) + 8 * c;
-        ld32B(src, x[k >> 1][k & 1][0]);
-        ld32B(src + 32, x[k >> 1][k & 1][1]);
+        const unsigned* src = spectra + sbase + (size_t)gk * (NF / 4) * 64;
+        if constexpr (FI == 4) {
+          ld32B(src, x[k >> 1][k & 1][0]);
+          ld32B(src + 32, x[k >> 1][k & 1][1]);
+        } else {
+          ld16B(src, x[k >> 1][k & 1][0]);
+          ld16B(src + 32, x[k >> 1][k & 1][1]);
+        }
       }
       const int stg = s % H16_S, sb = s % H16_NB, sbp = (s / H16_NB) & 1;
       ok = h16_stepG<H16_G, SD>(li, d, sx, fc, tile, dm, dirs, my_items, ntiles);
@@ -379,7 +401,7 @@ __global__ void __launch_bounds__(h16_threads(H16_G), 1)
 #pragma unroll
       for (int h = 0; h < 2; h++)
 #pragma unroll
-        for (int L = 0; L < 2; L++) {
+        for (int L = 0; L < FI / 2; L++) {
           unsigned r[16];
 #pragma unroll
           for (int i = 0; i < 4; i++) {
@@ -388,7 +410,7 @@ __global__ void __launch_bounds__(h16_threads(H16_G), 1)
             r[4 * i + 2] = x[h][1][0][4 * L + i];
             r[4 * i + 3] = x[h][1][1][4 * L + i];
           }
-          tmem_st16x256_x4(abase + (unsigned)stg * H16_ACOLS + ((unsigned)(16 * h) << 16) + 32 * L, r);
+          tmem_st16x256_x4(abase + (unsigned)stg * ACOLS + ((unsigned)(16 * h) << 16) + 32 * L, r);
         }
       asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -403,17 +425,16 @@ __global__ void __launch_bounds__(h16_threads(H16_G), 1)
     // after a time-out: the copy this warp issued last has landed before the CTA ends
     if (pend >= 0) mbar_wait_bounded(smem_u32(&bfull[pend % H16_NB]), (pend / H16_NB) & 1, H16_LONG_WAIT);
   } else {
-    // ---- MMA warps: warp H16_MMA_WARP + f issues frequency f's 2 MMAs of
-    // every step (own accumulator columns, one elected lane) and commits;
+    // ---- MMA warps: warp H16_MMA_WARP + w issues the 2 MMAs of every
+    // step for the accumulators kk = t FI + f = w, w + 4, ... (target dof t,
+    // frequency f; own accumulator columns, one elected lane) and commits;
     // the next step's afull is tested without blocking before this step's
     // MMAs go out.  At an item's end each drains TMEM lane quarter
-    // (warp mod 4), all four frequencies, into effval.
-    const int f = warp - H16_MMA_WARP;
+    // (warp mod 4), every accumulator, into effval.
+    const int w = warp - H16_MMA_WARP;
     const float inv_sa = inv_data_scale(__uint_as_float(*bound));
     int s = 0;
     bool ready = false, failed = false;
-    // A_hi of frequency f: column block 2 f, A_lo block 2 f + 1
-    const unsigned acol = H16_ACOL0 + 16 * f;
     for (int li = 0; li < my_items; li++) {
       const int nst = __popc(dirs[li]) * SD;
       for (int k = 0; k < nst; k++) {
@@ -429,8 +450,11 @@ __global__ void __launch_bounds__(h16_threads(H16_G), 1)
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const int s1 = s + 1;
         ready = mbar_test(smem_u32(&afull[s1 % H16_S]), (s1 / H16_S) & 1);
-        mma_freq16(tmem + f * 32, tmem + acol + (unsigned)stg * H16_ACOLS,
-                   img_desc16(smem_u32(imgs + (size_t)(s % H16_NB) * H16_IMG_BYTES + f * 1024)), k == 0 ? 0 : 1);
+        // A_hi of frequency f: column block 2 f, A_lo block 2 f + 1
+#pragma unroll
+        for (int kk = w; kk < TD * FI; kk += 4)
+          mma_freq16(tmem + kk * 32, tmem + ACOL0 + 16 * (kk % FI) + (unsigned)stg * ACOLS,
+                     img_desc16(smem_u32(imgs + (size_t)(s % H16_NB) * IMGB + kk * 1024)), k == 0 ? 0 : 1);
         commit_elect(smem_u32(&aempty[stg]));
         s++;
       }
@@ -440,38 +464,53 @@ __global__ void __launch_bounds__(h16_threads(H16_G), 1)
       if (!wait(&accfull, li & 1)) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const int i = blockIdx.x + li * gridDim.x;
-      const int ft = i / ntiles, tile = i - ft * ntiles;
-      const int fc = TD == 1 ? ft : ft / TD, tdf = TD == 1 ? 0 : ft - fc * TD;
+      const int fc = i / ntiles, tile = i - fc * ntiles;
+      const int fc4 = FI == 4 ? fc : fc >> 1;  // the 4-frequency block
       const int row = (warp & 3) * 32 + lane;
       const unsigned lane_off = (unsigned)((warp & 3) * 32) << 16;
       const int q = tile * H16_M + row;
-      const float scl = inv_sa * __ldg(inv_sb + fc);
-      // frequency f2: head*head + tail*head in columns 32 f2 + 0-15,
-      // head*tail in 32 f2 + 16-31; y[f2][2 i + (re, im)] of child i
-      float y[H16_F][16];
+      const float scl = inv_sa * __ldg(inv_sb + fc4);
+      const size_t gblk = q < nq ? ((size_t)((qchd[q] + 7) >> 3) * (NF / 4) + fc4) * 64 : 0;
+#pragma unroll 1
+      for (int t = 0; t < TD; t++) {
+        // frequency f2: head*head + tail*head in columns 32 kk + 0-15,
+        // head*tail in 32 kk + 16-31; y[f2][2 i + (re, im)] of child i
+        float y[FI][16];
 #pragma unroll
-      for (int f2 = 0; f2 < H16_F; f2++) {
-        unsigned r[16];
-        tmem_ld16(tmem + lane_off + f2 * 32, r);
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        for (int f2 = 0; f2 < FI; f2++) {
+          unsigned r[16];
+          const unsigned col = (unsigned)(t * FI + f2) * 32;
+          tmem_ld16(tmem + lane_off + col, r);
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-        for (int n = 0; n < 16; n++) y[f2][n] = __uint_as_float(r[n]);
-        tmem_ld16(tmem + lane_off + f2 * 32 + 16, r);
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+          for (int n = 0; n < 16; n++) y[f2][n] = __uint_as_float(r[n]);
+          tmem_ld16(tmem + lane_off + col + 16, r);
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-        for (int n = 0; n < 16; n++) y[f2][n] = (y[f2][n] + __uint_as_float(r[n])) * scl;
-      }
-      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-      asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&accempty)) : "memory");
-      // the row's 8 children x 4 frequencies: one 256-byte block of the
-      // sibling-group-major accumulated spectra (all 8 children; the inverse
-      // pass reads only the V-list targets among them)
-      if (q < nq) {
-        float* dst = effval + (TD == 1 ? 0 : tdf * plane * 2) + (((size_t)((qchd[q] + 7) >> 3) * (NF / H16_F) + fc) * 64);
+          for (int n = 0; n < 16; n++) y[f2][n] = (y[f2][n] + __uint_as_float(r[n])) * scl;
+        }
+        if (t == TD - 1) {
+          asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+          asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&accempty)) : "memory");
+        }
+        // the row's 8 children x 4 frequencies are one 256-byte block of the
+        // sibling-group-major accumulated spectra of dof t (all 8 children;
+        // the inverse pass reads only the V-list targets among them); FI = 2
+        // writes half of each child's 32 bytes
+        if (q < nq) {
+          float* dst = effval + (TD == 1 ? 0 : (size_t)t * plane * 2) + gblk;
+          if constexpr (FI == 4) {
 #pragma unroll
-        for (int ch = 0; ch < 8; ch++)
-          st32B(dst + 8 * ch, y[0][2 * ch], y[0][2 * ch + 1], y[1][2 * ch], y[1][2 * ch + 1], y[2][2 * ch],
-                y[2][2 * ch + 1], y[3][2 * ch], y[3][2 * ch + 1]);
+            for (int ch = 0; ch < 8; ch++)
+              st32B(dst + 8 * ch, y[0][2 * ch], y[0][2 * ch + 1], y[1][2 * ch], y[1][2 * ch + 1], y[2][2 * ch],
+                    y[2][2 * ch + 1], y[3][2 * ch], y[3][2 * ch + 1]);
+          } else {
+#pragma unroll
+            for (int ch = 0; ch < 8; ch++)
+              *reinterpret_cast<float4*>(dst + 8 * ch + (fc & 1) * 4) =
+                  make_float4(y[0][2 * ch], y[0][2 * ch + 1], y[1][2 * ch], y[1][2 * ch + 1]);
+          }
+        }
       }
     }
     // before the CTA ends every MMA issued has completed (only a time-out
@@ -527,10 +566,10 @@ void had_tc16_launch_g(const unsigned char* img, const unsigned* spectra, int nq
                        const unsigned* tile_dirs, float* effval, size_t plane, const unsigned* bound,
                        const float* inv_sb, int wait_limit, int* status, int num_sms, cudaStream_t st) {
   const int ntiles = (nq + H16_M - 1) / H16_M;
-  const int nitems = ntiles * (NF / H16_F) * TD;
+  const int nitems = ntiles * (NF / H16Shape<TD>::FI);
   if (nitems == 0) return;
   const int grid = std::min(num_sms, nitems);
-  const size_t smem = h16_smem((nitems + grid - 1) / grid);
+  const size_t smem = h16_smem(H16Shape<TD>::IMGB, (nitems + grid - 1) / grid);
   auto kern = k_m2l_had_tc16<NF, G, SD, TD>;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   kern<<<grid, h16_threads(G), smem, st>>>(img, spectra, nq, ntiles, qchd, ctab, tile_dirs, effval, nitems, plane,
@@ -574,14 +613,16 @@ bool m2l_tc16_supported(int nf, int sd, int td) {
 
 void m2l_tc16_images(int nf, int sd, int td, const std::complex<double>* m2l, std::vector<unsigned short>* img,
                      std::vector<float>* inv_sb) {
-  const int nch = nf / H16_F, nts = sd * td;
-  img->assign((size_t)nch * 26 * nts * (H16_IMG_BYTES / 2), 0);
+  const int fi = td == 1 ? 4 : 2;  // frequencies per work item (H16Shape)
+  const int nch = nf / 4, ncf = nf / fi, nts = sd * td;
+  img->assign((size_t)nf * 26 * nts * 512, 0);  // [chunk of fi][dir][s][t][fi] x 512 fp16
   inv_sb->assign(nch, 1.f);
   for (int fc = 0; fc < nch; fc++) {
-    // the chunk's scale (all dof pairs): 2^(14 - e) with every |entry| <= 2^e
+    // the scale of each block of 4 frequencies (all dof pairs): 2^(14 - e)
+    // with every |entry| <= 2^e
     double mx = 0;
     for (size_t o = 0; o < (size_t)343 * nts; o++)
-      for (int f = fc * H16_F; f < fc * H16_F + H16_F; f++) {
+      for (int f = fc * 4; f < fc * 4 + 4; f++) {
         const std::complex<double> t = m2l[o * nf + f];
         mx = std::max(mx, std::max(std::abs(t.real()), std::abs(t.imag())));
       }
@@ -598,28 +639,32 @@ void m2l_tc16_images(int nf, int sd, int td, const std::complex<double>* m2l, st
                             2 * dv[2] + (j & 1) - (i & 1)};
           if (std::max(std::abs(o[0]), std::max(std::abs(o[1]), std::abs(o[2]))) <= 1) continue;  // adjacent
           const int oi = (o[0] + 3) * 49 + (o[1] + 3) * 7 + (o[2] + 3);
-          for (int ts = 0; ts < nts; ts++)  // operator [343][td][sd][nf], image [chunk][dir][td][sd]
-            for (int fl = 0; fl < H16_F; fl++) {
-            const std::complex<double> t = m2l[((size_t)oi * nts + ts) * nf + fc * H16_F + fl] * sb;
-            // rows 2i + (re, im), columns 2j + (re, im): [[re, -im], [im, re]]
-            const double b[2][2] = {{t.real(), -t.imag()}, {t.imag(), t.real()}};
-            unsigned short* blk = img->data() + (((size_t)fc * 26 + dir) * nts + ts) * (H16_IMG_BYTES / 2) + fl * 512;
-            for (int a = 0; a < 2; a++)
-              for (int cc = 0; cc < 2; cc++) {
-                // K order of the A rows: column 2 c + e of a block = child c + 4 e
-                const int n = 2 * i + a, k = 2 * (2 * (j & 3) + (j >> 2)) + cc;
-                const __half hi = __float2half_rn((float)b[a][cc]);
-                const __half lo = __float2half_rn((float)(b[a][cc] - (double)__half2float(hi)));
-                // (row, k): K-adjacent core matrices 512 B apart, row groups
-                // of 8 128 B apart, rows 16 B apart; rows 16-31 hold the tails
-                auto at = [&](int row) { return (k / 8) * 256 + (row / 8) * 64 + (row % 8) * 8 + (k % 8); };
-                blk[at(n)] = __half_as_ushort(hi);
-                blk[at(16 + n)] = __half_as_ushort(lo);
+          for (int t = 0; t < td; t++)
+            for (int sx = 0; sx < sd; sx++)
+              for (int f = fc * 4; f < fc * 4 + 4; f++) {  // operator [343][td][sd][nf]
+                const std::complex<double> v = m2l[((size_t)oi * nts + t * sd + sx) * nf + f] * sb;
+                // rows 2i + (re, im), columns 2j + (re, im): [[re, -im], [im, re]]
+                const double b[2][2] = {{v.real(), -v.imag()}, {v.imag(), v.real()}};
+                const int cf = f / fi, fl = f % fi;
+                unsigned short* blk =
+                    img->data() + (((((size_t)cf * 26 + dir) * sd + sx) * td + t) * fi + fl) * 512;
+                for (int a = 0; a < 2; a++)
+                  for (int cc = 0; cc < 2; cc++) {
+                    // K order of the A rows: column 2 c + e of a block = child c + 4 e
+                    const int n = 2 * i + a, k = 2 * (2 * (j & 3) + (j >> 2)) + cc;
+                    const __half hi = __float2half_rn((float)b[a][cc]);
+                    const __half lo = __float2half_rn((float)(b[a][cc] - (double)__half2float(hi)));
+                    // (row, k): K-adjacent core matrices 512 B apart, row groups
+                    // of 8 128 B apart, rows 16 B apart; rows 16-31 hold the tails
+                    auto at = [&](int row) { return (k / 8) * 256 + (row / 8) * 64 + (row % 8) * 8 + (k % 8); };
+                    blk[at(n)] = __half_as_ushort(hi);
+                    blk[at(16 + n)] = __half_as_ushort(lo);
+                  }
               }
-          }
         }
     }
   }
+  (void)ncf;
 }
 
 void launch_spectra_bound(const float* supeden, const int* nodes, int n, const int* depth, int rootlvl,
