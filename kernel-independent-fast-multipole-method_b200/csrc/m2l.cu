@@ -73,6 +73,12 @@ __host__ __device__ inline size_t inv_rb_warp_bytes(int np, int n, int nh) {
   return align16(sizeof(Cpx<T>) * np * n * nh) + align16(sizeof(Cpx<T>) * np * np * nh);
 }
 
+// the staged accumulated spectrum of one node (sibling-group-major FP32 form)
+template <typename T>
+__host__ __device__ inline size_t inv_rb_stage_bytes(int np) {
+  return align16(sizeof(Cpx<T>) * (4 * np * np * np + 4));
+}
+
 template <typename T>
 __host__ __device__ inline size_t inv_warp_bytes(int np, int n, int nh) {
   return align16(sizeof(Cpx<T>) * n * n * nh) + align16(sizeof(Cpx<T>) * np * n * nh) +
@@ -511,10 +517,14 @@ __global__ void __launch_bounds__(256) k_m2l_inv_rb(M2LGeom g, const T* __restri
   __syncthreads();
   for (int m = threadIdx.x; m < NSURF; m += blockDim.x)
     m_of[(g.surf_ijk[3 * m] * NP + g.surf_ijk[3 * m + 1]) * NP + g.surf_ijk[3 * m + 2]] = m;
-  unsigned char* mine =
-      smem_raw + align16(sizeof(int) * (N * N * NH + NP * NP * NP)) + (size_t)warp * inv_rb_warp_bytes<T>(NP, N, NH);
+  // the sibling-group-major FP32 form stages each node's spectrum first
+  constexpr bool kStage = sizeof(T) == 4;
+  const bool stage_sg = kStage && g.effval_sg;
+  const size_t per_warp = inv_rb_warp_bytes<T>(NP, N, NH) + (stage_sg ? inv_rb_stage_bytes<T>(NP) : 0);
+  unsigned char* mine = smem_raw + align16(sizeof(int) * (N * N * NH + NP * NP * NP)) + (size_t)warp * per_warp;
   Cpx<T>* Bm = reinterpret_cast<Cpx<T>*>(mine);
   Cpx<T>* A = reinterpret_cast<Cpx<T>*>(mine + align16(sizeof(Cpx<T>) * NP * N * NH));
+  Cpx<T>* stage = reinterpret_cast<Cpx<T>*>(mine + inv_rb_warp_bytes<T>(NP, N, NH));
   __syncthreads();
   for (int wi = blockIdx.x * wpc + warp; wi < nwork; wi += gridDim.x * wpc) {
     const int node = work[wi];
@@ -522,8 +532,24 @@ __global__ void __launch_bounds__(256) k_m2l_inv_rb(M2LGeom g, const T* __restri
     for (int t = 0; t < g.td; t++) {
       const Cpx<T>* src = reinterpret_cast<const Cpx<T>*>(effval + ((size_t)node * g.td + t) * NFC * 2);
       // sibling-group-major accumulated spectra: value c of dof t at
-      // t * plane + spectra_sg_index
+      // t * plane + spectra_sg_index; the node's 4 values of each chunk of 4
+      // frequencies (32 bytes at a 256-byte stride) are copied into the
+      // warp's stage all at once, so the warp waits for memory once per node
+      // (the stage was last read by the previous z pass, which ends in a
+      // __syncwarp)
       const Cpx<T>* srcg = reinterpret_cast<const Cpx<T>*>(effval) + t * g.plane + spectra_sg_index(NFC, node, 0);
+      if constexpr (kStage) {
+        if (stage_sg) {
+          for (int b = lane; b < NFC / 4; b += 32) {
+            const unsigned d0 = (unsigned)__cvta_generic_to_shared(stage + 4 * b);
+            const Cpx<T>* s0 = srcg + 32 * b;
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d0), "l"(s0) : "memory");
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d0 + 16), "l"(s0 + 2) : "memory");
+          }
+          asm volatile("cp.async.wait_all;" ::: "memory");
+          __syncwarp();
+        }
+      }
       // z pass (inverse), lines (ky, kx): Bm[k][ky][kx] = sum_kz Y[kz][ky][kx] w^(-k kz), k < np
       for (int line = lane; line < N * NH; line += 32) {
         const int kx = line % NH, ky = line / NH;
@@ -532,7 +558,7 @@ __global__ void __launch_bounds__(256) k_m2l_inv_rb(M2LGeom g, const T* __restri
         for (int kz = 0; kz < N; kz++) {
           const int c = c_of[(kz * N + ky) * NH + kx];
           const int ca = c >= 0 ? c : -c - 1;
-          Cpx<T> v = g.effval_sg ? srcg[(ca >> 2) * 32 + (ca & 3)] : src[ca];
+          Cpx<T> v = stage_sg ? stage[ca] : g.effval_sg ? srcg[(ca >> 2) * 32 + (ca & 3)] : src[ca];
           if (c < 0) v.im = -v.im;
           y[kz] = v;
         }
@@ -640,7 +666,8 @@ void launch_m2l_inverse(const M2LGeom& g, const T* effval, const int* work, int 
   size_t smem = head + per_warp * wpc;
   int grid = std::max(1, std::min((nwork + wpc - 1) / wpc, 148 * 8));
   if (g.np == 4 || g.np == 6 || g.np == 8) {
-    const size_t per_rb = inv_rb_warp_bytes<T>(g.np, g.n, g.nh);
+    const size_t per_rb =
+        inv_rb_warp_bytes<T>(g.np, g.n, g.nh) + (sizeof(T) == 4 && g.effval_sg ? inv_rb_stage_bytes<T>(g.np) : 0);
     const size_t head_rb = align16(sizeof(int) * (g.n * g.n * g.nh + g.np * g.np * g.np));
     const int w = (int)std::max<size_t>(1, std::min<size_t>(8, (200 * 1024 - head_rb) / per_rb));
     const size_t sm = head_rb + per_rb * w;
