@@ -6,12 +6,10 @@ Tolerances (stated per test):
     acceptance rule for this path), plus agreement with the reference's
     eval output to the same bound.
   * mixed engine (FP32 bulk, FP64 pseudo-inverse products): relative error
-    <= max(10 x the reference's error, 1e-5) for the single-layer kernels
-    (111, 311, 511: the accuracy class the mixed engine is specified for),
-    and <= max(10 x the reference's error, 1e-3) for the double-layer and
-    pressure kernels, whose near-field sums cancel strongly and carry the
-    FP32 rounding of those sums (e.g. 8e-5 for 322 on a sphere, where the
-    reference's own FMM error is 2.5e-10).
+    <= max(10 x the reference's error, 1e-5) for every kernel; the
+    double-layer and pressure kernels, whose near-field sums cancel
+    strongly, sum their U lists in FP64 (e.g. kernel 322 on a sphere:
+    2.5e-10, the reference's own error).
   * direct sum on the device vs the oracle: 1e-12 relative.
 """
 import numpy as np
@@ -26,7 +24,6 @@ pytestmark = pytest.mark.gpu
 
 FP64_FACTOR = 10.0
 MIXED_FLOOR = 1e-5
-MIXED_FLOOR_DL = 1e-3
 
 
 def engine_for(d, precision):
@@ -65,8 +62,7 @@ def test_mixed_matches_reference(gpu, name):
     _, out = eval_case(d, "mixed")
     td = W.KERNEL_DOFS[d["kt"]][1]
     err = oracle.relerr(out.reshape(-1, td)[d["chk"]], d["ref_direct"])
-    floor = MIXED_FLOOR if d["kt"] in (111, 311, 511) else MIXED_FLOOR_DL
-    assert err <= max(FP64_FACTOR * d["ref_relerr"], floor), (err, d["ref_relerr"])
+    assert err <= max(FP64_FACTOR * d["ref_relerr"], MIXED_FLOOR), (err, d["ref_relerr"])
 
 
 @pytest.mark.parametrize("kt", [111, 121, 311, 312, 321, 322, 511, 521])
