@@ -363,7 +363,10 @@ def batched_section(torch, kifmm, stream, flush, steps, warmup, precision, pg=No
             times.append(e0.elapsed_time(e1))
         if b is not None:
             b.poll_status()  # a device-side wait that timed out in a timed replay raises here
-        launches = int(sum(f.last_launch_count() for f in fmms))
+        # kernel launches of one replay: instances sharing kernel, np,
+        # precision, schedule and root level run as one concatenated forest
+        binfo = b.info() if b is not None else {"units": 0, "forests": 0, "launches": 0}
+        launches = binfo["launches"]
         errs = []
         for inst, f, den, p, out in zip(insts, fmms, dens, pts, outs):
             n = inst["n"]
@@ -381,6 +384,7 @@ def batched_section(torch, kifmm, stream, flush, steps, warmup, precision, pg=No
             k = f'{inst["kt"]}:g{sc["had_groups"]}:c{sc["rhs_chunk"]}'
             tuned[k] = tuned.get(k, 0) + 1
         return statistics.mean(times), {"errs": errs, "setup_s": setup_s, "launches": launches,
+                                        "units": binfo["units"], "forests": binfo["forests"],
                                         "schedules": tuned,
                                         "tuned_fresh": sum(1 for sc in scheds if not sc["from_cache"])}
 
@@ -414,6 +418,7 @@ def batched_section(torch, kifmm, stream, flush, steps, warmup, precision, pg=No
             "max_ratio_to_reference_error": ratio,
             "setup_s": extra["setup_s"], "launches_per_step": extra["launches"],
             "autotuned_schedules": extra["schedules"], "schedules_tuned_fresh": extra["tuned_fresh"],
+            "graph_units": extra["units"], "concatenated_forests": extra["forests"],
             "points_per_instance_total": sum(i["n"] for i in insts_all), "instances_this_rank": len(res["mine"]),
             "lpt_imbalance": res["imbalance"]}
 

@@ -119,11 +119,26 @@ kifmm_status kifmm_poll_status(kifmm_handle h);
  * A batch groups already set-up handles (any kernels and sizes); each
  * kifmm_batch_eval_device call evaluates nrhs density vectors for every
  * instance (device pointers d_srcden[i] / d_trgval[i], layouts as in
- * kifmm_eval_device).  The instances run concurrently, and the whole batch is
- * captured into one CUDA graph on the first call and replayed while nrhs and
- * the pointers stay the same. */
+ * kifmm_eval_device).  Instances with the same kernel, np, precision,
+ * V-list form, schedule and root level are concatenated at creation into one
+ * forest (their trees side by side, their points one after another), so each
+ * pass of the evaluation is one launch over all of them; their results agree
+ * with a kifmm_eval_device per instance to rounding (the summation order of
+ * some passes changes with the merged work lists; the mixed engine's FP16
+ * scale is shared by the forest).  Forests and the remaining instances run
+ * concurrently, and the whole batch is captured into one CUDA graph on the
+ * first call and replayed while nrhs and the pointers stay the same.  The
+ * forest holds its own device copy of the members' set-up data. */
 typedef struct kifmm_batch_s* kifmm_batch;
 kifmm_status kifmm_batch_create(int n, const kifmm_handle* handles, kifmm_batch* out);
+/* kifmm_batch_create with concatenate = 0: every instance evaluated by its own
+ * engine on its own stream (each result bit-identical to its own
+ * kifmm_eval_device). */
+kifmm_status kifmm_batch_create_opts(int n, const kifmm_handle* handles, int concatenate, kifmm_batch* out);
+/* The batch's units (forests + single instances), forests among them, and the
+ * kernel launches of one replay of the captured evaluation (0 before the
+ * first kifmm_batch_eval_device). */
+kifmm_status kifmm_batch_info(kifmm_batch b, int* nunits, int* nforests, int* launches);
 kifmm_status kifmm_batch_destroy(kifmm_batch b);
 kifmm_status kifmm_batch_eval_device(kifmm_batch b, int nrhs, const double* const* d_srcden,
                                      double* const* d_trgval, void* stream, int sync);

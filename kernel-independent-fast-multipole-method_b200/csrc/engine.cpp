@@ -16,6 +16,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <mutex>
 #include <random>
@@ -1492,6 +1493,200 @@ int Engine::autotune_run() {
     g_tuned[key] = best;
   }
   finish(best, false);
+  return KIFMM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Concatenated instances.  Member trees go side by side: for every depth,
+// each member's nodes of that depth as one block in its own breadth-first
+// order, every block at depth >= 1 starting at an id that is 1 mod 8 (empty
+// padding nodes fill the gaps), so every sibling group stays one aligned
+// group of 8 and the forest's ids are breadth first again (depth never
+// decreases).  Lists, parents and children are renumbered; point ranges are
+// shifted by the member's point offset.  Padding nodes carry no points, no
+// tag and no lists, so no pass touches them.
+namespace {
+void merge_trees(const std::vector<const Tree*>& ts, const std::vector<int>& soff, const std::vector<int>& toff,
+                 Tree& t) {
+  const int K = (int)ts.size();
+  int md = 0;
+  for (auto* x : ts) md = std::max(md, x->maxdepth);
+  std::vector<std::vector<int>> map(K);
+  for (int k = 0; k < K; k++) map[k].assign(ts[k]->nnodes, -1);
+  std::vector<int> from_k, from_old;  // per forest node: member and its id there (-1: padding)
+  std::vector<int> pad_depth;
+  t.level_beg.clear();
+  for (int d = 0; d <= md; d++) {
+    t.level_beg.push_back((int)from_k.size());
+    for (int k = 0; k < K; k++) {
+      const Tree& x = *ts[k];
+      if (d > x.maxdepth) continue;
+      const int lb = x.level_beg[d], le = x.level_beg[d + 1];
+      if (le <= lb) continue;
+      if (d >= 1)
+        while (from_k.size() % 8 != 1) {
+          from_k.push_back(-1);
+          from_old.push_back(d);
+        }
+      for (int g = lb; g < le; g++) {
+        map[k][g] = (int)from_k.size();
+        from_k.push_back(k);
+        from_old.push_back(g);
+      }
+    }
+  }
+  t.level_beg.push_back((int)from_k.size());
+  const int n = (int)from_k.size();
+  t.nnodes = n;
+  t.maxdepth = md;
+  t.ctr[0] = ts[0]->ctr[0];
+  t.ctr[1] = ts[0]->ctr[1];
+  t.ctr[2] = ts[0]->ctr[2];
+  t.rootlvl = ts[0]->rootlvl;
+  t.ptsmax = ts[0]->ptsmax;
+  t.maxlevel = ts[0]->maxlevel;
+  t.depth.assign(n, 0);
+  t.par.assign(n, -1);
+  t.chd.assign(n, -1);
+  t.tag.assign(n, 0);
+  t.path.assign(3 * (size_t)n, 0);
+  t.sbeg.assign(n, 0);
+  t.scnt.assign(n, 0);
+  t.tbeg.assign(n, 0);
+  t.tcnt.assign(n, 0);
+  t.center.assign(3 * (size_t)n, 0.0);
+  t.radius.assign(n, 0.0);
+  for (int g = 0; g < n; g++) {
+    const int k = from_k[g];
+    if (k < 0) {
+      t.depth[g] = from_old[g];
+      continue;
+    }
+    const Tree& x = *ts[k];
+    const int o = from_old[g];
+    t.depth[g] = x.depth[o];
+    t.par[g] = x.par[o] >= 0 ? map[k][x.par[o]] : -1;
+    t.chd[g] = x.chd[o] >= 0 ? map[k][x.chd[o]] : -1;
+    t.tag[g] = x.tag[o];
+    for (int a = 0; a < 3; a++) {
+      t.path[3 * (size_t)g + a] = x.path[3 * (size_t)o + a];
+      t.center[3 * (size_t)g + a] = x.center[3 * (size_t)o + a];
+    }
+    t.sbeg[g] = x.sbeg[o] + soff[k];
+    t.scnt[g] = x.scnt[o];
+    t.tbeg[g] = x.tbeg[o] + toff[k];
+    t.tcnt[g] = x.tcnt[o];
+    t.radius[g] = x.radius[o];
+  }
+  t.sperm.clear();
+  t.tperm.clear();
+  for (int k = 0; k < K; k++) {
+    for (int p : ts[k]->sperm) t.sperm.push_back(p + soff[k]);
+    for (int p : ts[k]->tperm) t.tperm.push_back(p + toff[k]);
+  }
+  for (int w = 0; w < 4; w++) {
+    Csr& c = t.lists[w];
+    c.ptr.assign(1, 0);
+    c.idx.clear();
+    for (int g = 0; g < n; g++) {
+      const int k = from_k[g];
+      if (k >= 0) {
+        const Csr& xc = ts[k]->lists[w];
+        const int o = from_old[g];
+        for (int64_t e = xc.ptr[o]; e < xc.ptr[o + 1]; e++) c.idx.push_back(map[k][xc.idx[e]]);
+      }
+      c.ptr.push_back((int64_t)c.idx.size());
+    }
+  }
+}
+}  // namespace
+
+std::string Engine::forest_key() const {
+  if (!ready || per_level || !tree_ready) return std::string();
+  char b[320];
+  std::snprintf(b, sizeof b, "%d %.17g %.17g %d %d %d %d %d %d %d %d %d %d %d", user.kt, user.coefs[0], user.coefs[1],
+                mm.kt, np, mixed ? 1 : 0, tensor_cores ? 1 : 0, m2l_toeplitz ? 1 : 0, m2l_tc ? 1 : 0,
+                m2l_tc_tf32 ? 1 : 0, had_groups, rhs_chunk, rootlvl, wait_limit);
+  return std::string(b);
+}
+
+int Engine::setup_forest(const std::vector<const Engine*>& ms) {
+  ready = false;
+  if (ms.empty()) {
+    err = "no members";
+    return KIFMM_ERR_ARG;
+  }
+  const Engine& m0 = *ms[0];
+  const std::string key = m0.forest_key();
+  for (const Engine* m : ms)
+    if (key.empty() || m->forest_key() != key) {
+      err = "members differ in kernel, np, precision, schedule or root level";
+      return KIFMM_ERR_ARG;
+    }
+  prefix = m0.prefix;
+  opts = m0.opts;
+  np = m0.np;
+  ptsmax = m0.ptsmax;
+  maxlevel = m0.maxlevel;
+  mixed = m0.mixed;
+  tensor_cores = m0.tensor_cores;
+  m2l_toeplitz = m0.m2l_toeplitz;
+  m2l_tc = m0.m2l_tc;
+  m2l_tc_tf32 = m0.m2l_tc_tf32;
+  wait_limit = m0.wait_limit;
+  had_groups = m0.had_groups;
+  rhs_chunk = m0.rhs_chunk;
+  per_level = false;
+  user = m0.user;
+  mm = m0.mm;
+  have_kernel = true;
+  rootlvl = m0.rootlvl;
+  for (int a = 0; a < 3; a++) ctr[a] = m0.ctr[a];
+  ops = m0.ops;
+  src_off.clear();
+  trg_off.clear();
+  ns = nt = 0;
+  srcpos.clear();
+  srcnor.clear();
+  trgpos.clear();
+  std::vector<const Tree*> ts;
+  for (const Engine* m : ms) {
+    src_off.push_back(ns);
+    trg_off.push_back(nt);
+    ns += m->ns;
+    nt += m->nt;
+    srcpos.insert(srcpos.end(), m->srcpos.begin(), m->srcpos.end());
+    srcnor.insert(srcnor.end(), m->srcnor.begin(), m->srcnor.end());
+    trgpos.insert(trgpos.end(), m->trgpos.begin(), m->trgpos.end());
+    ts.push_back(&m->tree);
+  }
+  have_geom = true;
+  release_device();
+  tree = Tree();
+  merge_trees(ts, src_off, trg_off, tree);
+  tree_ready = true;
+  device = m0.device;
+  try {
+    if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess) throw CudaError{cudaGetLastError(), "stream"};
+    if (mixed) {
+      auto p = std::make_unique<Impl<float>>(*this);
+      p->build();
+      impl = std::move(p);
+    } else {
+      auto p = std::make_unique<Impl<double>>(*this);
+      p->build();
+      impl = std::move(p);
+    }
+    KCHECK(cudaDeviceSynchronize());
+  } catch (const CudaError& e) {
+    err = std::string(e.where) + ": " + cudaGetErrorString(e.e);
+    cudaGetLastError();
+    release_device();
+    return e.e == cudaErrorMemoryAllocation ? KIFMM_ERR_ALLOC : KIFMM_ERR_CUDA;
+  }
+  schedule[0] = had_groups;
+  schedule[1] = rhs_chunk;
+  ready = true;
   return KIFMM_OK;
 }
 

@@ -90,6 +90,17 @@ struct Engine {
   int setup();  // returns a kifmm_status
   // times the candidate schedules on the set-up engine (autotune option)
   int autotune_run();
+  // Instances that can share one concatenated forest engine give the same
+  // key (kernel, equivalent kernel, np, precision, V-list form, schedule,
+  // root level, wait limit); empty for instances that cannot be merged.
+  std::string forest_key() const;
+  // Sets this engine up as the concatenation of set-up members with one
+  // forest_key: their trees side by side (node ids level by level, every
+  // sibling group kept aligned), their points one after another, one work
+  // list per pass over all of them.  Member k's sources are points
+  // [src_off[k], src_off[k] + ns_k) of the forest, its targets likewise.
+  int setup_forest(const std::vector<const Engine*>& members);
+  std::vector<int> src_off, trg_off;
   int eval_host(const double* srcden, double* trgval, int nrhs);
   int eval_device(const double* d_srcden, double* d_trgval, int nrhs, cudaStream_t st, bool sync);
   // Enqueues the evaluation passes on st without any host synchronisation

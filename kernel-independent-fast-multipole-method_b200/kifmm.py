@@ -65,6 +65,8 @@ SIGNATURES = {
     "kifmm_work_counters": [_H, _DP, _IP],
     "kifmm_last_launch_count": [_H, _IP],
     "kifmm_batch_create": [ctypes.c_int, ctypes.POINTER(_H), ctypes.POINTER(ctypes.c_void_p)],
+    "kifmm_batch_create_opts": [ctypes.c_int, ctypes.POINTER(_H), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)],
+    "kifmm_batch_info": [ctypes.c_void_p, _IP, _IP, _IP],
     "kifmm_batch_destroy": [ctypes.c_void_p],
     "kifmm_batch_eval_device": [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
                                 ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p, ctypes.c_int],
@@ -308,13 +310,21 @@ class Batch:
     (kifmm_batch_*): eval(srcden_ptrs, trgval_ptrs, nrhs, stream) takes one
     device pointer pair per instance."""
 
-    def __init__(self, fmms):
+    def __init__(self, fmms, concatenate: bool = True):
         self.fmms = list(fmms)
         hs = (_H * len(self.fmms))(*[f._h for f in self.fmms])
         self._b = ctypes.c_void_p()
-        st = lib().kifmm_batch_create(len(self.fmms), hs, ctypes.byref(self._b))
+        st = lib().kifmm_batch_create_opts(len(self.fmms), hs, 1 if concatenate else 0, ctypes.byref(self._b))
         if st != 0:
             raise KifmmError(st, "kifmm_batch_create failed")
+
+    def info(self):
+        """kifmm_batch_info: units, forests among them, kernel launches per replay."""
+        u, f, l = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        st = lib().kifmm_batch_info(self._b, ctypes.byref(u), ctypes.byref(f), ctypes.byref(l))
+        if st != 0:
+            raise KifmmError(st, "kifmm_batch_info failed")
+        return {"units": u.value, "forests": f.value, "launches": l.value}
 
     def eval(self, d_srcden, d_trgval, nrhs: int = 1, stream: int = 0, sync: bool = True) -> int:
         n = len(self.fmms)

@@ -1,9 +1,13 @@
 """Batched evaluation (kifmm_batch_*): several set-up instances, of different
 kernels and precisions, evaluated in one captured CUDA graph.
 
-The graph replays exactly the passes a single eval_device enqueues, so each
-instance's output must be bit-identical to its own eval_device call; a new
-set of buffers or rhs count recaptures the graph.
+Without concatenation the graph replays exactly the passes a single
+eval_device enqueues, so each instance's output must be bit-identical to its
+own eval_device call; a new set of buffers or rhs count recaptures the
+graph.  Instances that share kernel, np, precision, schedule and root level
+are concatenated into one forest engine (one launch per pass for all of
+them): equal to their single evals to rounding (1e-12 relative in FP64, 1e-6
+in mixed precision, whose FP16 spectra scale the forest shares).
 """
 import numpy as np
 import pytest
@@ -44,7 +48,7 @@ def test_batch_matches_single_instance_evals(gpu):
         srcs.append(s)
         outs.append(o)
         want.append(ref.cpu().numpy())
-    b = kifmm.Batch(fmms)
+    b = kifmm.Batch(fmms, concatenate=False)
     for _ in range(2):  # capture, then replay
         for o in outs:
             o.zero_()
@@ -73,3 +77,50 @@ def test_batch_rejects_bad_arguments(gpu):
     unset = kifmm.FMM3d("fmm3d_")
     with pytest.raises(kifmm.KifmmError):
         kifmm.Batch([unset])
+
+
+def _cloud_engine(kt, n, geometry, seed, precision):
+    p, _ = W.GEOMETRIES[geometry](n, seed)
+    f = kifmm.FMM3d("fmm3d_")
+    f.srcpos = f.srcnor = f.trgpos = p
+    f.knl = kifmm.Kernel3d(kt, [1.0, 0.25])
+    f.setup({"-fmm3d_np": "6", "-fmm3d_let3d_ptsmax": "64", "-fmm3d_let3d_maxlevel": "10",
+             "-fmm3d_precision": precision})
+    return f
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("mixed", 1e-6)])
+def test_concatenated_instances_match_single_instance_evals(gpu, precision, tol):
+    """Five Laplace instances (one with separate source and target sets and
+    its own root box) and two Stokes instances: two forests, each one launch
+    per pass; every instance's potentials equal its own eval to rounding."""
+    torch = pytest.importorskip("torch")
+    nrhs = 3
+    fmms = [_cloud_engine(111, 4000, "sphere", 1, precision), _cloud_engine(111, 9000, "cube", 2, precision),
+            _cloud_engine(111, 6000, "plummer_ball", 3, precision), _cloud_engine(111, 2500, "cube", 4, precision),
+            _cloud_engine(311, 5000, "cube", 5, precision), _cloud_engine(311, 3000, "sphere", 6, precision)]
+    d = G.load("lap_s_np6_tt_style")
+    t = _engine(d, precision)
+    fmms.insert(2, t)
+    rng = np.random.default_rng(5)
+    srcs, outs, want, single_launches = [], [], [], 0
+    for f in fmms:
+        den = rng.uniform(-1, 1, nrhs * f.sdof() * f.ns)
+        s = torch.tensor(den, device="cuda", dtype=torch.float64)
+        ref = torch.zeros(nrhs * f.tdof() * f.nt, device="cuda", dtype=torch.float64)
+        f.eval_device(s.data_ptr(), ref.data_ptr(), nrhs, 0, sync=True)
+        single_launches += f.last_launch_count()
+        srcs.append(s)
+        outs.append(torch.zeros_like(ref))
+        want.append(ref.cpu().numpy())
+    b = kifmm.Batch(fmms)
+    for _ in range(2):  # capture, then replay
+        for o in outs:
+            o.zero_()
+        b.eval([s.data_ptr() for s in srcs], [o.data_ptr() for o in outs], nrhs, 0, sync=True)
+        for f, o, w in zip(fmms, outs, want):
+            got = o.cpu().numpy()
+            assert np.linalg.norm(got - w) <= tol * np.linalg.norm(w), (f.knl.kt, np.linalg.norm(got - w) / np.linalg.norm(w))
+    info = b.info()
+    assert info["forests"] == 2 and info["units"] == 2
+    assert 0 < info["launches"] < single_launches / 2
