@@ -361,6 +361,32 @@ __global__ void __launch_bounds__(h16_threads(H16_G), 1)
     g3 = __ldg(tb + 24);                                              \
   }
     if (ok) H16_LOAD_G()
+    // x[h][ab][e][w] = word w (frequency w / 2 of the chunk, {hi, lo} =
+    // w % 2) of child c + 4 e of the colleague of row (h, ab); a child's 4
+    // frequencies of a 256-byte block are 8 words, FI = 2 takes half of them
+    unsigned x[2][2][2][2 * FI];
+    // the loads of half h of the step at the iterator's position (its
+    // colleague groups in g0 .. g3)
+#define H16_LOAD_HALF(h)                                                                                  \
+  {                                                                                                       \
+    const size_t sbase = (SD == 1 ? 0 : sx * plane * 2) + (size_t)(FI == 4 ? fc : fc >> 1) * 64 + 8 * c + \
+                         (FI == 4 ? 0 : (fc & 1) * 4);                                                    \
+    _Pragma("unroll") for (int ab = 0; ab < 2; ab++) {                                                    \
+      const int gk = (h) == 0 ? (ab == 0 ? g0 : g1) : (ab == 0 ? g2 : g3);                                \
+      const unsigned* src = spectra + sbase + (size_t)gk * (NF / 4) * 64;                                 \
+      if constexpr (FI == 4) {                                                                            \
+        ld32B(src, x[h][ab][0]);                                                                          \
+        ld32B(src + 32, x[h][ab][1]);                                                                     \
+      } else {                                                                                            \
+        ld16B(src, x[h][ab][0]);                                                                          \
+        ld16B(src + 32, x[h][ab][1]);                                                                     \
+      }                                                                                                   \
+    }                                                                                                     \
+  }
+    if (ok) {
+      H16_LOAD_HALF(0)
+      H16_LOAD_HALF(1)
+    }
     int s = grp, pend = -1;  // pend: step of an operator copy not yet seen landed
     while (ok) {
       // the step's operator images into stage s mod NB, last read by step
@@ -371,35 +397,20 @@ __global__ void __launch_bounds__(h16_threads(H16_G), 1)
         bulk_load(smem_u32(imgs + (size_t)(s % H16_NB) * IMGB), img + (((size_t)fc * 26 + d) * SD + sx) * IMGB, IMGB,
                   smem_u32(&bfull[s % H16_NB]));
       if (qd == 0) pend = s;
-      // all of the step's loads at once: x[h][ab][e][w] = word w
-      // (frequency w / 2 of the chunk, {hi, lo} = w % 2) of child c + 4 e of
-      // the colleague of row (h, ab), so the step waits for memory once; a
-      // child's 4 frequencies of a 256-byte block are 8 words, FI = 2 takes
-      // half of them
-      unsigned x[2][2][2][2 * FI];
-      const size_t sbase = (SD == 1 ? 0 : sx * plane * 2) + (size_t)(FI == 4 ? fc : fc >> 1) * 64 + 8 * c +
-                           (FI == 4 ? 0 : (fc & 1) * 4);
-#pragma unroll
-      for (int k = 0; k < 4; k++) {
-        const int gk = k == 0 ? g0 : k == 1 ? g1 : k == 2 ? g2 : g3;
-        const unsigned* src = spectra + sbase + (size_t)gk * (NF / 4) * 64;
-        if constexpr (FI == 4) {
-          ld32B(src, x[k >> 1][k & 1][0]);
-          ld32B(src + 32, x[k >> 1][k & 1][1]);
-        } else {
-          ld16B(src, x[k >> 1][k & 1][0]);
-          ld16B(src + 32, x[k >> 1][k & 1][1]);
-        }
-      }
       const int stg = s % H16_S, sb = s % H16_NB, sbp = (s / H16_NB) & 1;
-      ok = h16_stepG<H16_G, SD>(li, d, sx, fc, tile, dm, dirs, my_items, ntiles);
-      if (ok) H16_LOAD_G()  // the g's are free once the step's loads are issued
+      // the iterator moves to the group's next step and its colleague groups
+      // are requested; the step's own data is already in x
+      const bool nxt = h16_stepG<H16_G, SD>(li, d, sx, fc, tile, dm, dirs, my_items, ntiles);
+      if (nxt) H16_LOAD_G()
       if (s >= H16_S && !wait(&aempty[stg], ((s / H16_S) + 1) & 1)) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       // column block b = 2 f + {hi, lo}; in every block column 2c + e holds
-      // child c + 4e; one store per half h and pair of frequencies L
+      // child c + 4e; one store per half h and pair of frequencies L.  Each
+      // half's registers take the next step's loads as soon as its stores
+      // are issued, so those loads are in flight through this step's store
+      // wait, image wait and arrive
 #pragma unroll
-      for (int h = 0; h < 2; h++)
+      for (int h = 0; h < 2; h++) {
 #pragma unroll
         for (int L = 0; L < FI / 2; L++) {
           unsigned r[16];
@@ -412,6 +423,13 @@ __global__ void __launch_bounds__(h16_threads(H16_G), 1)
           }
           tmem_st16x256_x4(abase + (unsigned)stg * ACOLS + ((unsigned)(16 * h) << 16) + 32 * L, r);
         }
+        if (nxt) {
+          if (h == 0)
+            H16_LOAD_HALF(0)
+          else
+            H16_LOAD_HALF(1)
+        }
+      }
       asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       if (qd == 0) {
@@ -420,7 +438,9 @@ __global__ void __launch_bounds__(h16_threads(H16_G), 1)
       }
       asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&afull[stg])) : "memory");
       s += H16_G;
+      ok = nxt;
     }
+#undef H16_LOAD_HALF
 #undef H16_LOAD_G
     // after a time-out: the copy this warp issued last has landed before the CTA ends
     if (pend >= 0) mbar_wait_bounded(smem_u32(&bfull[pend % H16_NB]), (pend / H16_NB) & 1, H16_LONG_WAIT);
