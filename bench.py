@@ -364,7 +364,7 @@ def batched_section(torch, kifmm, stream, flush, steps, warmup, precision, pg=No
         if b is not None:
             b.poll_status()  # a device-side wait that timed out in a timed replay raises here
         # kernel launches of one replay: instances sharing kernel, np,
-        # precision, schedule and root level run as one concatenated forest
+        # precision, V-list form and root level run as one concatenated forest
         binfo = b.info() if b is not None else {"units": 0, "forests": 0, "launches": 0}
         launches = binfo["launches"]
         errs = []

@@ -120,7 +120,7 @@ kifmm_status kifmm_poll_status(kifmm_handle h);
  * kifmm_batch_eval_device call evaluates nrhs density vectors for every
  * instance (device pointers d_srcden[i] / d_trgval[i], layouts as in
  * kifmm_eval_device).  Instances with the same kernel, np, precision,
- * V-list form, schedule and root level are concatenated at creation into one
+ * V-list form and root level are concatenated at creation into one
  * forest (their trees side by side, their points one after another), so each
  * pass of the evaluation is one launch over all of them; their results agree
  * with a kifmm_eval_device per instance to rounding (the summation order of

@@ -3,7 +3,7 @@
 // one CUDA graph.  The reference evaluates one instance at a time on one CPU
 // thread (fmm3d/tt.cpp:97-101).
 //
-// Instances that share kernel, np, precision, schedule and root level
+// Instances that share kernel, np, precision, V-list form and root level
 // (Engine::forest_key) are concatenated into one forest engine: their trees
 // side by side, their points one after another, so every pass of the eval is
 // ONE launch over the work queues of all of them (leaf lists, V-list parent

@@ -1603,10 +1603,13 @@ void merge_trees(const std::vector<const Tree*>& ts, const std::vector<int>& sof
 
 std::string Engine::forest_key() const {
   if (!ready || per_level || !tree_ready) return std::string();
+  // (the schedule knobs -- producer groups, density vectors per pass --
+  // change no result, so members may have tuned them differently; the
+  // forest takes its first member's)
   char b[320];
-  std::snprintf(b, sizeof b, "%d %.17g %.17g %d %d %d %d %d %d %d %d %d %d %d", user.kt, user.coefs[0], user.coefs[1],
-                mm.kt, np, mixed ? 1 : 0, tensor_cores ? 1 : 0, m2l_toeplitz ? 1 : 0, m2l_tc ? 1 : 0,
-                m2l_tc_tf32 ? 1 : 0, had_groups, rhs_chunk, rootlvl, wait_limit);
+  std::snprintf(b, sizeof b, "%d %.17g %.17g %d %d %d %d %d %d %d %d %d", user.kt, user.coefs[0], user.coefs[1], mm.kt,
+                np, mixed ? 1 : 0, tensor_cores ? 1 : 0, m2l_toeplitz ? 1 : 0, m2l_tc ? 1 : 0, m2l_tc_tf32 ? 1 : 0,
+                rootlvl, wait_limit);
   return std::string(b);
 }
 
@@ -1620,7 +1623,7 @@ int Engine::setup_forest(const std::vector<const Engine*>& ms) {
   const std::string key = m0.forest_key();
   for (const Engine* m : ms)
     if (key.empty() || m->forest_key() != key) {
-      err = "members differ in kernel, np, precision, schedule or root level";
+      err = "members differ in kernel, np, precision, V-list form or root level";
       return KIFMM_ERR_ARG;
     }
   prefix = m0.prefix;

@@ -91,8 +91,8 @@ struct Engine {
   // times the candidate schedules on the set-up engine (autotune option)
   int autotune_run();
   // Instances that can share one concatenated forest engine give the same
-  // key (kernel, equivalent kernel, np, precision, V-list form, schedule,
-  // root level, wait limit); empty for instances that cannot be merged.
+  // key (kernel, equivalent kernel, np, precision, V-list form, root level,
+  // wait limit); empty for instances that cannot be merged.
   std::string forest_key() const;
   // Sets this engine up as the concatenation of set-up members with one
   // forest_key: their trees side by side (node ids level by level, every

@@ -4,7 +4,7 @@ kernels and precisions, evaluated in one captured CUDA graph.
 Without concatenation the graph replays exactly the passes a single
 eval_device enqueues, so each instance's output must be bit-identical to its
 own eval_device call; a new set of buffers or rhs count recaptures the
-graph.  Instances that share kernel, np, precision, schedule and root level
+graph.  Instances that share kernel, np, precision, V-list form and root level
 are concatenated into one forest engine (one launch per pass for all of
 them): equal to their single evals to rounding (1e-12 relative in FP64, 1e-6
 in mixed precision, whose FP16 spectra scale the forest shares).
