@@ -124,3 +124,36 @@ def test_concatenated_instances_match_single_instance_evals(gpu, precision, tol)
     info = b.info()
     assert info["forests"] == 2 and info["units"] == 2
     assert 0 < info["launches"] < single_launches / 2
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("mixed", 1e-6)])
+def test_concatenated_double_layer_instances(gpu, precision, tol):
+    """Double-layer instances (Stokes 321 and Navier 521, with normals) in
+    forests: in mixed precision their U lists run in FP64 through the
+    forest's own FP64 near-field pass."""
+    torch = pytest.importorskip("torch")
+    fmms = []
+    for kt, n, geo, seed in ((321, 3000, "sphere", 7), (321, 5000, "ellipsoid", 8), (521, 2500, "sphere", 9),
+                             (521, 4000, "sphere", 10)):
+        p, nor = W.GEOMETRIES[geo](n, seed)
+        f = kifmm.FMM3d("fmm3d_")
+        f.srcpos, f.srcnor, f.trgpos = p, nor, p
+        f.knl = kifmm.Kernel3d(kt, [1.0, 0.3])
+        f.setup({"-fmm3d_np": "4", "-fmm3d_let3d_ptsmax": "60", "-fmm3d_let3d_maxlevel": "10",
+                 "-fmm3d_precision": precision})
+        fmms.append(f)
+    rng = np.random.default_rng(9)
+    srcs, outs, want = [], [], []
+    for f in fmms:
+        s = torch.tensor(rng.uniform(-1, 1, 2 * f.sdof() * f.ns), device="cuda", dtype=torch.float64)
+        ref = torch.zeros(2 * f.tdof() * f.nt, device="cuda", dtype=torch.float64)
+        f.eval_device(s.data_ptr(), ref.data_ptr(), 2, 0, sync=True)
+        srcs.append(s)
+        outs.append(torch.zeros_like(ref))
+        want.append(ref.cpu().numpy())
+    b = kifmm.Batch(fmms)
+    b.eval([s.data_ptr() for s in srcs], [o.data_ptr() for o in outs], 2, 0, sync=True)
+    assert b.info()["forests"] == 2
+    for f, o, w in zip(fmms, outs, want):
+        got = o.cpu().numpy()
+        assert np.linalg.norm(got - w) <= tol * np.linalg.norm(w), (f.knl.kt, np.linalg.norm(got - w) / np.linalg.norm(w))
