@@ -92,10 +92,18 @@ constexpr int H16_LONG_WAIT = 1 << 22;           // polls of the end-of-CTA wait
 template <int TD>
 struct H16Shape {
   static constexpr int FI = TD == 1 ? 4 : 2;
-  static constexpr unsigned ACOL0 = TD * FI * 32;
-  static constexpr unsigned ACOLS = FI * 16;
-  static constexpr unsigned IMGB = TD * FI * 1024;
+  // source dofs per step: a multi-dof step carries a pair (the A stage then
+  // holds 2 dofs x 2 frequencies, the bytes of one single-dof step), and its
+  // accumulators are 16 columns (the head*tail product is a third N = 16
+  // MMA instead of the upper half of an N = 32 one)
+  static constexpr int SPS = TD == 1 ? 1 : 2;
+  static constexpr unsigned ACC = TD == 1 ? 32 : 16;
+  static constexpr unsigned ACOL0 = TD * FI * ACC;
+  static constexpr unsigned ACOLS = SPS * FI * 16;
+  static constexpr unsigned IMGB = SPS * TD * FI * 1024;
 };
+// steps per colleague direction: the source-dof pairs
+constexpr int h16_dof_steps(int SD, int TD) { return TD == 1 ? SD : (SD + 1) / 2; }
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 
@@ -164,6 +172,26 @@ __device__ __forceinline__ void mma_freq16(unsigned d, unsigned a, uint64_t b, i
       " @e tcgen05.mma.cta_group::1.kind::f16 [%0], [a], %2, %5, t;\n"
       "}\n" ::"r"(d),
       "r"(a), "l"(b), "r"(acc), "r"(idesc_f16<32>()), "r"(idesc_f16<16>())
+      : "memory");
+}
+
+// one (target dof, frequency, source dof) block product of a multi-dof step
+// into its N = 16 accumulator: D (+)= A_hi B_hi^T + A_lo B_hi^T + A_hi B_lo^T
+// (A_lo 8 columns after A_hi, B_lo the image's rows 16-31)
+__device__ __forceinline__ void mma3_16(unsigned d, unsigned a, uint64_t bhi, uint64_t blo, int acc) {
+  asm volatile(
+      "{\n"
+      " .reg .pred e, p, t;\n"
+      " .reg .b32 a;\n"
+      " setp.ne.b32 p, %4, 0;\n"
+      " setp.eq.b32 t, %4, %4;\n"
+      " elect.sync _|e, 0xffffffff;\n"
+      " @e tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %5, p;\n"
+      " add.u32 a, %1, 8;\n"
+      " @e tcgen05.mma.cta_group::1.kind::f16 [%0], [a], %2, %5, t;\n"
+      " @e tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %3, %5, t;\n"
+      "}\n" ::"r"(d),
+      "r"(a), "l"(bhi), "l"(blo), "r"(acc), "r"(idesc_f16<16>())
       : "memory");
 }
 
@@ -286,6 +314,7 @@ __global__ void __launch_bounds__(h16_threads(H16_G), 1)
   constexpr int H16_NB = H16_G + H16_S;    // operator image stages: step s uses s mod NB
   constexpr int FI = H16Shape<TD>::FI;
   constexpr unsigned ACOL0 = H16Shape<TD>::ACOL0, ACOLS = H16Shape<TD>::ACOLS, IMGB = H16Shape<TD>::IMGB;
+  constexpr int SDS = h16_dof_steps(SD, TD);  // steps per direction (source dofs or their pairs)
   static_assert(ACOL0 + H16_S * ACOLS <= H16_COLS, "A stages fit in TMEM");
   static_assert(H16_NB <= H16_NBI, "image stages");
   extern __shared__ __align__(1024) unsigned char smem[];
@@ -348,7 +377,7 @@ __global__ void __launch_bounds__(h16_threads(H16_G), 1)
     int li = 0, d = -1, sx = SD - 1, fc = blockIdx.x / ntiles, tile = blockIdx.x - fc * ntiles;
     unsigned dm = dirs[0];
     bool ok = true;
-    for (int k = 0; k <= grp && ok; k++) ok = h16_step<SD>(li, d, sx, fc, tile, dm, dirs, my_items, ntiles);
+    for (int k = 0; k <= grp && ok; k++) ok = h16_step<SDS>(li, d, sx, fc, tile, dm, dirs, my_items, ntiles);
     // the colleague groups of this thread's 4 rows at the group's next step,
     // loaded one group step ahead of their use
     int g0 = 0, g1 = 0, g2 = 0, g3 = 0;
@@ -364,22 +393,34 @@ __global__ void __launch_bounds__(h16_threads(H16_G), 1)
     // x[h][ab][e][w] = word w (frequency w / 2 of the chunk, {hi, lo} =
     // w % 2) of child c + 4 e of the colleague of row (h, ab); a child's 4
     // frequencies of a 256-byte block are 8 words, FI = 2 takes half of them
-    unsigned x[2][2][2][2 * FI];
+    unsigned x[2][2][2][8];
     // the loads of half h of the step at the iterator's position (its
     // colleague groups in g0 .. g3)
 #define H16_LOAD_HALF(h)                                                                                  \
   {                                                                                                       \
-    const size_t sbase = (SD == 1 ? 0 : sx * plane * 2) + (size_t)(FI == 4 ? fc : fc >> 1) * 64 + 8 * c + \
-                         (FI == 4 ? 0 : (fc & 1) * 4);                                                    \
-    _Pragma("unroll") for (int ab = 0; ab < 2; ab++) {                                                    \
-      const int gk = (h) == 0 ? (ab == 0 ? g0 : g1) : (ab == 0 ? g2 : g3);                                \
-      const unsigned* src = spectra + sbase + (size_t)gk * (NF / 4) * 64;                                 \
-      if constexpr (FI == 4) {                                                                            \
+    if constexpr (TD == 1) {                                                                              \
+      const size_t sbase = (size_t)fc * 64 + 8 * c;                                                       \
+      _Pragma("unroll") for (int ab = 0; ab < 2; ab++) {                                                  \
+        const int gk = (h) == 0 ? (ab == 0 ? g0 : g1) : (ab == 0 ? g2 : g3);                              \
+        const unsigned* src = spectra + sbase + (size_t)gk * (NF / 4) * 64;                               \
         ld32B(src, x[h][ab][0]);                                                                          \
         ld32B(src + 32, x[h][ab][1]);                                                                     \
-      } else {                                                                                            \
+      }                                                                                                   \
+    } else {                                                                                              \
+      /* source dofs 2 sx and 2 sx + 1 (zero past the last): words 0-3 and 4-7 */                         \
+      const size_t sbase = (size_t)(2 * sx) * plane * 2 + (size_t)(fc >> 1) * 64 + 8 * c + (fc & 1) * 4;  \
+      const bool two = 2 * sx + 1 < SD;                                                                   \
+      _Pragma("unroll") for (int ab = 0; ab < 2; ab++) {                                                  \
+        const int gk = (h) == 0 ? (ab == 0 ? g0 : g1) : (ab == 0 ? g2 : g3);                              \
+        const unsigned* src = spectra + sbase + (size_t)gk * (NF / 4) * 64;                               \
         ld16B(src, x[h][ab][0]);                                                                          \
         ld16B(src + 32, x[h][ab][1]);                                                                     \
+        if (two) {                                                                                        \
+          ld16B(src + plane * 2, x[h][ab][0] + 4);                                                        \
+          ld16B(src + plane * 2 + 32, x[h][ab][1] + 4);                                                   \
+        } else {                                                                                          \
+          _Pragma("unroll") for (int q = 4; q < 8; q++) x[h][ab][0][q] = x[h][ab][1][q] = 0u;             \
+        }                                                                                                 \
       }                                                                                                   \
     }                                                                                                     \
   }
@@ -394,25 +435,26 @@ __global__ void __launch_bounds__(h16_threads(H16_G), 1)
       // s - G - S complete, and NB = G + S
       // images [chunk][direction][source dof][target dof][frequency]
       if (qd == 0 && lane == 0)
-        bulk_load(smem_u32(imgs + (size_t)(s % H16_NB) * IMGB), img + (((size_t)fc * 26 + d) * SD + sx) * IMGB, IMGB,
+        bulk_load(smem_u32(imgs + (size_t)(s % H16_NB) * IMGB), img + (((size_t)fc * 26 + d) * SDS + sx) * IMGB, IMGB,
                   smem_u32(&bfull[s % H16_NB]));
       if (qd == 0) pend = s;
       const int stg = s % H16_S, sb = s % H16_NB, sbp = (s / H16_NB) & 1;
       // the iterator moves to the group's next step and its colleague groups
       // are requested; the step's own data is already in x
-      const bool nxt = h16_stepG<H16_G, SD>(li, d, sx, fc, tile, dm, dirs, my_items, ntiles);
+      const bool nxt = h16_stepG<H16_G, SDS>(li, d, sx, fc, tile, dm, dirs, my_items, ntiles);
       if (nxt) H16_LOAD_G()
       if (s >= H16_S && !wait(&aempty[stg], ((s / H16_S) + 1) & 1)) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      // column block b = 2 f + {hi, lo}; in every block column 2c + e holds
-      // child c + 4e; one store per half h and pair of frequencies L.  Each
+      // column block b = 2 f + {hi, lo} (f over the frequencies, or over the
+      // pair's dofs x frequencies); in every block column 2c + e holds
+      // child c + 4e; one store per half h and 4 column blocks L.  Each
       // half's registers take the next step's loads as soon as its stores
       // are issued, so those loads are in flight through this step's store
       // wait, image wait and arrive
 #pragma unroll
       for (int h = 0; h < 2; h++) {
 #pragma unroll
-        for (int L = 0; L < FI / 2; L++) {
+        for (int L = 0; L < 2; L++) {
           unsigned r[16];
 #pragma unroll
           for (int i = 0; i < 4; i++) {
@@ -456,7 +498,7 @@ __global__ void __launch_bounds__(h16_threads(H16_G), 1)
     int s = 0;
     bool ready = false, failed = false;
     for (int li = 0; li < my_items; li++) {
-      const int nst = __popc(dirs[li]) * SD;
+      const int nst = __popc(dirs[li]) * SDS;
       for (int k = 0; k < nst; k++) {
         const int stg = s % H16_S;
         if (!__all_sync(0xffffffffu, ready) && !wait(&afull[stg], (s / H16_S) & 1)) {
@@ -471,10 +513,28 @@ __global__ void __launch_bounds__(h16_threads(H16_G), 1)
         const int s1 = s + 1;
         ready = mbar_test(smem_u32(&afull[s1 % H16_S]), (s1 / H16_S) & 1);
         // A_hi of frequency f: column block 2 f, A_lo block 2 f + 1
+        if constexpr (TD == 1) {
 #pragma unroll
-        for (int kk = w; kk < TD * FI; kk += 4)
-          mma_freq16(tmem + kk * 32, tmem + ACOL0 + 16 * (kk % FI) + (unsigned)stg * ACOLS,
-                     img_desc16(smem_u32(imgs + (size_t)(s % H16_NB) * IMGB + kk * 1024)), k == 0 ? 0 : 1);
+          for (int kk = w; kk < FI; kk += 4)
+            mma_freq16(tmem + kk * 32, tmem + ACOL0 + 16 * kk + (unsigned)stg * ACOLS,
+                       img_desc16(smem_u32(imgs + (size_t)(s % H16_NB) * IMGB + kk * 1024)), k == 0 ? 0 : 1);
+        } else {
+          // accumulator kk = t FI + f; the pair's dof L = 0, 1 (the second
+          // only where it exists): A blocks 2 (L FI + f) + {hi, lo}, images
+          // [L][t][f]
+          const int sp = k % SDS;
+          const unsigned ib = smem_u32(imgs + (size_t)(s % H16_NB) * IMGB);
+#pragma unroll
+          for (int kk = w; kk < TD * FI; kk += 4) {
+#pragma unroll
+            for (int L = 0; L < 2; L++) {
+              if (L == 1 && 2 * sp + 1 >= SD) break;
+              const unsigned b = ib + (unsigned)((L * TD + kk / FI) * FI + kk % FI) * 1024u;
+              mma3_16(tmem + kk * 16, tmem + ACOL0 + 16 * (L * FI + kk % FI) + (unsigned)stg * ACOLS,
+                      img_desc16(b), img_desc16(b + 256), (k == 0 && L == 0) ? 0 : 1);
+            }
+          }
+        }
         commit_elect(smem_u32(&aempty[stg]));
         s++;
       }
@@ -499,15 +559,19 @@ __global__ void __launch_bounds__(h16_threads(H16_G), 1)
 #pragma unroll
         for (int f2 = 0; f2 < FI; f2++) {
           unsigned r[16];
-          const unsigned col = (unsigned)(t * FI + f2) * 32;
+          const unsigned col = (unsigned)(t * FI + f2) * H16Shape<TD>::ACC;
           tmem_ld16(tmem + lane_off + col, r);
           asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
           for (int n = 0; n < 16; n++) y[f2][n] = __uint_as_float(r[n]);
-          tmem_ld16(tmem + lane_off + col + 16, r);
-          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+          if constexpr (TD == 1) {  // + the head*tail half
+            tmem_ld16(tmem + lane_off + col + 16, r);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-          for (int n = 0; n < 16; n++) y[f2][n] = (y[f2][n] + __uint_as_float(r[n])) * scl;
+            for (int n = 0; n < 16; n++) y[f2][n] += __uint_as_float(r[n]);
+          }
+#pragma unroll
+          for (int n = 0; n < 16; n++) y[f2][n] *= scl;
         }
         if (t == TD - 1) {
           asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -634,8 +698,11 @@ bool m2l_tc16_supported(int nf, int sd, int td) {
 void m2l_tc16_images(int nf, int sd, int td, const std::complex<double>* m2l, std::vector<unsigned short>* img,
                      std::vector<float>* inv_sb) {
   const int fi = td == 1 ? 4 : 2;  // frequencies per work item (H16Shape)
+  // source-dof slots per direction: the dofs, rounded up to whole pairs for
+  // several dofs (a padding slot stays zero)
+  const int sds = td == 1 ? sd : (sd + 1) / 2 * 2;
   const int nch = nf / 4, ncf = nf / fi, nts = sd * td;
-  img->assign((size_t)nf * 26 * nts * 512, 0);  // [chunk of fi][dir][s][t][fi] x 512 fp16
+  img->assign((size_t)nf * 26 * sds * td * 512, 0);  // [chunk of fi][dir][s][t][fi] x 512 fp16
   inv_sb->assign(nch, 1.f);
   for (int fc = 0; fc < nch; fc++) {
     // the scale of each block of 4 frequencies (all dof pairs): 2^(14 - e)
@@ -667,7 +734,7 @@ void m2l_tc16_images(int nf, int sd, int td, const std::complex<double>* m2l, st
                 const double b[2][2] = {{v.real(), -v.imag()}, {v.imag(), v.real()}};
                 const int cf = f / fi, fl = f % fi;
                 unsigned short* blk =
-                    img->data() + (((((size_t)cf * 26 + dir) * sd + sx) * td + t) * fi + fl) * 512;
+                    img->data() + (((((size_t)cf * 26 + dir) * sds + sx) * td + t) * fi + fl) * 512;
                 for (int a = 0; a < 2; a++)
                   for (int cc = 0; cc < 2; cc++) {
                     // K order of the A rows: column 2 c + e of a block = child c + 4 e
