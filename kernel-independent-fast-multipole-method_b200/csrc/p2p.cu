@@ -375,9 +375,11 @@ __global__ void __launch_bounds__(32 * WP_WARPS) k_s2m_warp(P2PArgs<T> a, const 
   }
 }
 
-// Leaf pass: lane = (target slot, source split) with G = the power of two
-// >= the leaf's target count (<= 32) slots and 32 / G splits; splits are
-// summed with warp shuffles.  Sources are staged 32 at a time: point
+// Leaf pass: the leaf's targets in rounds of up to 32; in a round lane =
+// (target slot, source split) with G = the power of two >= the round's
+// target count (<= 32) slots and 32 / G splits, so a leaf of 33-64 targets
+// splits its last round's sources over the lanes its few targets leave;
+// splits are summed with warp shuffles.  Sources are staged 32 at a time: point
 // sources from the leaf's near list (segments = source leaves, found by
 // bisection of the warp's prefix sums), then the W-list upward equivalent
 // surfaces and the leaf's own downward equivalent surface.
@@ -417,10 +419,10 @@ __global__ void __launch_bounds__(32 * NWARP) k_leaf_warp(P2PArgs<T> a, const in
     const int64_t nb = nptr[wi], ne = nptr[wi + 1];
     const int64_t mb = mptr[wi], me = mptr[wi + 1];
     const int nsurf_segs = (int)(me - mb) + (l2t ? 1 : 0);
-    int G = 1;
-    while (G < nt && G < 32) G <<= 1;
-    const int nsplit = 32 / G, slot = lane % G, sg = lane / G;
-    for (int tb = 0; tb < nt; tb += G) {
+    for (int tb = 0, G = 32; tb < nt; tb += G) {
+      G = 1;
+      while (G < nt - tb && G < 32) G <<= 1;
+      const int nsplit = 32 / G, slot = lane % G, sg = lane / G;
       const int ti = tb + slot;
       const bool valid = ti < nt;
       T px = 0, py = 0, pz = 0;
